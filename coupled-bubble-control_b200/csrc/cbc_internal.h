@@ -1,0 +1,105 @@
+// cbc_internal.h -- host-side helpers shared by the translation units of
+// libcbc_b200.so (context, error reporting, parameter conversion).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <mutex>
+#include <string>
+
+#include "../../include/cbc_b200.h"
+#include "ckm1d_core.cuh"
+
+struct cbc_context {
+  int device = 0;
+  int sm_count = 0;
+  int* d_counter = nullptr;       // device: systems still active after a launch
+  int* h_counter = nullptr;       // pinned host mirror
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+};
+
+namespace cbc {
+
+// Message store for failures that happen without a context.
+inline std::string& global_error() {
+  static std::string s;
+  return s;
+}
+inline std::mutex& global_error_mutex() {
+  static std::mutex m;
+  return m;
+}
+
+inline int32_t fail(cbc_context* ctx, int32_t code, const char* fmt, ...) __attribute__((format(printf, 3, 4)));
+inline int32_t fail(cbc_context* ctx, int32_t code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  else {
+    std::lock_guard<std::mutex> lk(global_error_mutex());
+    global_error() = buf;
+  }
+  return code;
+}
+
+#define CBC_CUDA_TRY(ctx, call)                                                              \
+  do {                                                                                       \
+    cudaError_t e__ = (call);                                                                \
+    if (e__ != cudaSuccess)                                                                  \
+      return ::cbc::fail((ctx), CBC_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e__)); \
+  } while (0)
+
+inline Params make_params(const cbc_spec& s) {
+  Params p;
+  p.atol = s.atol;
+  p.rtol = s.rtol;
+  p.min_step = s.min_step;
+  p.max_step = s.max_step;
+  p.lin_atol2 = s.lin_atol * s.lin_atol;
+  p.lin_rtol2 = s.lin_rtol * s.lin_rtol;
+  p.omega = s.lin_relaxation;
+  p.etol = s.etol;
+  p.col = 1.0 + s.col_threshold;
+  p.lin_max_iter = s.lin_max_iter;
+  p.ndo = s.ndo;
+  p.dense_mode = s.dense_mode;
+  p.nk = s.nk;
+  p.ac = s.ac;
+  return p;
+}
+
+inline int32_t check_spec(cbc_context* ctx, const cbc_spec* s) {
+  if (!s) return fail(ctx, CBC_E_INVALID, "spec is NULL");
+  if (s->ns < 1) return fail(ctx, CBC_E_INVALID, "ns must be >= 1 (got %d)", s->ns);
+  if (s->ups < 1) return fail(ctx, CBC_E_INVALID, "ups must be >= 1 (got %d)", s->ups);
+  if (s->ups > 32) return fail(ctx, CBC_E_UNSUPPORTED, "ups = %d: at most 32 bubbles per system", s->ups);
+  if (s->tile < s->ups) return fail(ctx, CBC_E_INVALID, "tile (%d) < ups (%d)", s->tile, s->ups);
+  if (s->nk < 1 || s->nk > NKMAX)
+    return fail(ctx, CBC_E_UNSUPPORTED, "nk = %d: 1..%d harmonic components supported", s->nk, NKMAX);
+  if (s->ac < 0 || s->ac > 2) return fail(ctx, CBC_E_INVALID, "ac = %d: expected 0 CONST, 1 SW_N, 2 SW_A", s->ac);
+  if (s->ndo < 0) return fail(ctx, CBC_E_INVALID, "ndo must be >= 0");
+  if (s->dense_mode < 0 || s->dense_mode > 1) return fail(ctx, CBC_E_INVALID, "dense_mode must be 0 or 1");
+  if (s->lin_max_iter < 0) return fail(ctx, CBC_E_INVALID, "lin_max_iter must be >= 0");
+  if (!(s->min_step > 0.0) || !(s->max_step >= s->min_step))
+    return fail(ctx, CBC_E_INVALID, "need 0 < min_step <= max_step");
+  if (!(s->atol > 0.0) || !(s->rtol >= 0.0)) return fail(ctx, CBC_E_INVALID, "need atol > 0, rtol >= 0");
+  return CBC_OK;
+}
+
+// Smallest power-of-two instantiation that holds K bubbles per system.
+inline int kb_for(int K) {
+  if (K <= 2) return 2;
+  if (K <= 4) return 4;
+  if (K <= 8) return 8;
+  if (K <= 16) return 16;
+  return 32;
+}
+
+}  // namespace cbc

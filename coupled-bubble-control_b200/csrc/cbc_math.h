@@ -1,0 +1,238 @@
+// cbc_math.h -- FP64 elementary functions shared by the CUDA kernels and the
+// CPU oracle.
+//
+// Why not libm / CUDA's libdevice: the integrator is compared against its CPU
+// oracle bit for bit.  That only works if both sides evaluate sin, cos, exp and
+// log with the same operations in the same order.  These routines use only
+// IEEE-754 add, mul, fma, division and exact bit manipulation, so gcc (with
+// -ffp-contract=off) and nvcc (with -fmad=false) produce identical results.
+//
+// Methods (all published, coefficients are the exact Taylor coefficients
+// rounded to double, computed with mpmath; no vendor constants are used):
+//   * sin/cos: Cody & Waite additive argument reduction by pi/2 with a
+//     three-part split of pi/2 applied through fma (W. J. Cody, W. Waite,
+//     "Software Manual for the Elementary Functions", 1980, ch. 8), followed by
+//     Taylor polynomials on |r| <= pi/4 (sin to r^19, cos to r^18; truncation
+//     < 1e-19 relative).  Valid for |x| < 2^20 (accuracy degrades gracefully
+//     beyond); the integrator's phase arguments stay below 2e5.
+//   * exp: reduction x = n ln2 + r, |r| <= ln2/2, two-part ln2 through fma,
+//     Taylor polynomial to r^13 (truncation < 1e-17), scaling by 2^n built from
+//     the exponent bits (Cody & Waite ch. 6).
+//   * log: x = 2^e m, m in [sqrt(2)/2, sqrt(2)), log m = 2 atanh(f),
+//     f = (m-1)/(m+1), odd series to f^23 (Cody & Waite ch. 5).
+//   * pow(x, y) for x > 0 as exp(y log x).
+// Accuracy against glibc (checked by tests/test_cbc_math.py): sin/cos/exp/log
+// within 2 ulp; pow within ~1e-15 relative for |y log x| < 50.
+#pragma once
+
+#include <stdint.h>
+#include <math.h>
+#if !defined(__CUDACC__)
+#include <string.h>
+#endif
+
+#if defined(__CUDACC__)
+#define CBC_HD __host__ __device__ __forceinline__
+#else
+#define CBC_HD static inline
+#endif
+
+namespace cbcm {
+
+CBC_HD double bits_to_double(uint64_t u) {
+#if defined(__CUDA_ARCH__)
+  return __longlong_as_double((long long)u);
+#else
+  double d;
+  memcpy(&d, &u, sizeof(d));
+  return d;
+#endif
+}
+
+CBC_HD uint64_t double_to_bits(double d) {
+#if defined(__CUDA_ARCH__)
+  return (uint64_t)__double_as_longlong(d);
+#else
+  uint64_t u;
+  memcpy(&u, &d, sizeof(u));
+  return u;
+#endif
+}
+
+CBC_HD double fma_(double a, double b, double c) { return fma(a, b, c); }
+CBC_HD double rint_(double a) { return rint(a); }
+CBC_HD double fabs_(double a) { return fabs(a); }
+CBC_HD bool isfinite_(double a) {
+  // exponent field all ones <=> inf or nan
+  return ((double_to_bits(a) >> 52) & 0x7ff) != 0x7ff;
+}
+
+// pi/2 = PIO2_1 + PIO2_2 + PIO2_3 (each the nearest double of the remainder)
+static constexpr double PIO2_1 = 0x1.921fb54442d18p+0;
+static constexpr double PIO2_2 = 0x1.1a62633145c07p-54;
+static constexpr double PIO2_3 = -0x1.f1976b7ed8fbcp-110;
+static constexpr double TWO_OVER_PI = 0x1.45f306dc9c883p-1;
+
+// sin(r) = r + r z (S3 + z (S5 + ...)),  z = r^2,  S_n = (-1)^((n-1)/2) / n!
+static constexpr double S3 = -0x1.5555555555555p-3;
+static constexpr double S5 = 0x1.1111111111111p-7;
+static constexpr double S7 = -0x1.a01a01a01a01ap-13;
+static constexpr double S9 = 0x1.71de3a556c734p-19;
+static constexpr double S11 = -0x1.ae64567f544e4p-26;
+static constexpr double S13 = 0x1.6124613a86d09p-33;
+static constexpr double S15 = -0x1.ae7f3e733b81fp-41;
+static constexpr double S17 = 0x1.952c77030ad4ap-49;
+static constexpr double S19 = -0x1.2f49b46814157p-57;
+// cos(r) = 1 + z (C2 + z (C4 + ...)),  C_n = (-1)^(n/2) / n!
+static constexpr double C2 = -0x1.0000000000000p-1;
+static constexpr double C4 = 0x1.5555555555555p-5;
+static constexpr double C6 = -0x1.6c16c16c16c17p-10;
+static constexpr double C8 = 0x1.a01a01a01a01ap-16;
+static constexpr double C10 = -0x1.27e4fb7789f5cp-22;
+static constexpr double C12 = 0x1.1eed8eff8d898p-29;
+static constexpr double C14 = -0x1.93974a8c07c9dp-37;
+static constexpr double C16 = 0x1.ae7f3e733b81fp-45;
+static constexpr double C18 = -0x1.6827863b97d97p-53;
+
+// sin and cos of x together.  NaN/inf input gives NaN outputs.
+CBC_HD void sincos(double x, double* s, double* c) {
+  if (!isfinite_(x)) {
+    *s = x - x;  // NaN for +-inf and NaN
+    *c = *s;
+    return;
+  }
+  double kd = rint_(x * TWO_OVER_PI);
+  double r = fma_(-kd, PIO2_1, x);
+  r = fma_(-kd, PIO2_2, r);
+  r = fma_(-kd, PIO2_3, r);
+  double z = r * r;
+  double ps = fma_(S19, z, S17);
+  ps = fma_(ps, z, S15);
+  ps = fma_(ps, z, S13);
+  ps = fma_(ps, z, S11);
+  ps = fma_(ps, z, S9);
+  ps = fma_(ps, z, S7);
+  ps = fma_(ps, z, S5);
+  ps = fma_(ps, z, S3);
+  double sr = fma_(r * z, ps, r);
+  double pc = fma_(C18, z, C16);
+  pc = fma_(pc, z, C14);
+  pc = fma_(pc, z, C12);
+  pc = fma_(pc, z, C10);
+  pc = fma_(pc, z, C8);
+  pc = fma_(pc, z, C6);
+  pc = fma_(pc, z, C4);
+  pc = fma_(pc, z, C2);
+  double cr = fma_(z, pc, 1.0);
+  // quadrant q = k mod 4 from the low two bits of k (two's complement keeps
+  // k mod 4 in the low bits for negative k).
+  //   q=0: ( s,  c)   q=1: ( c, -s)   q=2: (-s, -c)   q=3: (-c,  s)
+  long long ki = (long long)kd;
+  int q = (int)(ki & 3);
+  double a = (q & 1) ? cr : sr;
+  double b = (q & 1) ? sr : cr;
+  *s = (q & 2) ? -a : a;
+  *c = ((q + 1) & 2) ? -b : b;
+}
+
+static constexpr double LOG2E = 0x1.71547652b82fep+0;
+static constexpr double LN2_HI = 0x1.62e42fefa39efp-1;
+static constexpr double LN2_LO = 0x1.abc9e3b39803fp-56;
+static constexpr double E2 = 0x1.0000000000000p-1;
+static constexpr double E3 = 0x1.5555555555555p-3;
+static constexpr double E4 = 0x1.5555555555555p-5;
+static constexpr double E5 = 0x1.1111111111111p-7;
+static constexpr double E6 = 0x1.6c16c16c16c17p-10;
+static constexpr double E7 = 0x1.a01a01a01a01ap-13;
+static constexpr double E8 = 0x1.a01a01a01a01ap-16;
+static constexpr double E9 = 0x1.71de3a556c734p-19;
+static constexpr double E10 = 0x1.27e4fb7789f5cp-22;
+static constexpr double E11 = 0x1.ae64567f544e4p-26;
+static constexpr double E12 = 0x1.1eed8eff8d898p-29;
+static constexpr double E13 = 0x1.6124613a86d09p-33;
+
+// 2^n for integer n in [-1022, 1023] (exact)
+CBC_HD double pow2i(int n) { return bits_to_double((uint64_t)(n + 1023) << 52); }
+
+CBC_HD double exp(double x) {
+  if (!(x < 709.8)) return (x != x) ? x : bits_to_double(0x7ff0000000000000ULL);
+  if (x < -745.2) return 0.0;
+  double nd = rint_(x * LOG2E);
+  double r = fma_(-nd, LN2_HI, x);
+  r = fma_(-nd, LN2_LO, r);
+  double p = fma_(E13, r, E12);
+  p = fma_(p, r, E11);
+  p = fma_(p, r, E10);
+  p = fma_(p, r, E9);
+  p = fma_(p, r, E8);
+  p = fma_(p, r, E7);
+  p = fma_(p, r, E6);
+  p = fma_(p, r, E5);
+  p = fma_(p, r, E4);
+  p = fma_(p, r, E3);
+  p = fma_(p, r, E2);
+  p = fma_(p, r, 1.0);
+  p = fma_(p, r, 1.0);
+  int n = (int)nd;
+  // split the scaling so that results in the subnormal range round once
+  if (n > 1000) return p * pow2i(1000) * pow2i(n - 1000);
+  if (n < -1000) return p * pow2i(-1000) * pow2i(n + 1000);
+  return p * pow2i(n);
+}
+
+static constexpr double SQRT1_2 = 0x1.6a09e667f3bcdp-1;
+static constexpr double L3 = 0x1.5555555555555p-2;
+static constexpr double L5 = 0x1.999999999999ap-3;
+static constexpr double L7 = 0x1.2492492492492p-3;
+static constexpr double L9 = 0x1.c71c71c71c71cp-4;
+static constexpr double L11 = 0x1.745d1745d1746p-4;
+static constexpr double L13 = 0x1.3b13b13b13b14p-4;
+static constexpr double L15 = 0x1.1111111111111p-4;
+static constexpr double L17 = 0x1.e1e1e1e1e1e1ep-5;
+static constexpr double L19 = 0x1.af286bca1af28p-5;
+static constexpr double L21 = 0x1.8618618618618p-5;
+static constexpr double L23 = 0x1.642c8590b2164p-5;
+
+CBC_HD double log(double x) {
+  if (!(x > 0.0)) {
+    if (x == 0.0) return -bits_to_double(0x7ff0000000000000ULL);
+    return bits_to_double(0x7ff8000000000000ULL);  // x < 0 or NaN
+  }
+  if (!isfinite_(x)) return x;  // +inf
+  int eadj = 0;
+  if (x < 0x1p-1022) {  // subnormal: scale into the normal range (exact)
+    x = x * 0x1p54;
+    eadj = -54;
+  }
+  uint64_t u = double_to_bits(x);
+  int e = (int)((u >> 52) & 0x7ff) - 1023;
+  // m in [1, 2)
+  double m = bits_to_double((u & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL);
+  if (m > 2.0 * SQRT1_2) {
+    m = m * 0.5;
+    e += 1;
+  }
+  e += eadj;
+  double f = (m - 1.0) / (m + 1.0);
+  double s = f * f;
+  double p = fma_(L23, s, L21);
+  p = fma_(p, s, L19);
+  p = fma_(p, s, L17);
+  p = fma_(p, s, L15);
+  p = fma_(p, s, L13);
+  p = fma_(p, s, L11);
+  p = fma_(p, s, L9);
+  p = fma_(p, s, L7);
+  p = fma_(p, s, L5);
+  p = fma_(p, s, L3);
+  double f2 = f + f;
+  double logm = fma_(f2 * s, p, f2);
+  double ed = (double)e;
+  return fma_(ed, LN2_HI, fma_(ed, LN2_LO, logm));
+}
+
+// x^y for x > 0 (x <= 0 gives NaN, matching the physical meaning of a
+// collapsed radius).
+CBC_HD double pow_pos(double x, double y) { return cbcm::exp(y * cbcm::log(x)); }
+
+}  // namespace cbcm

@@ -1,0 +1,204 @@
+// ensemble.cu -- batched mixed-K integrator: persistent, work-stealing kernels
+// over a ragged ensemble, launched together (optionally as one CUDA graph).
+//
+// The reference can only integrate one (NS, K) ensemble per kernel build
+// (all shapes are compile-time macros, backends/cupy_cuda/kernel_loader.py:35-63;
+// one thread per bubble padded to TILE = next_pow2(K), specs.py:40-52) and
+// relaunches every kernel_steps steps with a host synchronisation.  Here:
+//   * systems of any K <= 32 live in one ragged ensemble (CSR offsets);
+//   * a work list orders the systems by K bucket, longest expected work first;
+//   * each warp holds floor(32/K) system slots; whenever a system finishes,
+//     its slot writes the result back and claims the next system of its bucket
+//     with one atomicAdd per warp, so lanes never idle while work remains;
+//   * one persistent kernel per K bucket (instantiated for KB = 2,4,8,16,32
+//     lanes per system slot), launched on forked streams so the buckets overlap
+//     and a bucket's tail is filled by the next bucket's warps.
+// Integration arithmetic is the same device code as the reference-layout
+// kernel (ckm1d_core.cuh), so results are bit-identical to the CPU oracle.
+#include "cbc_internal.h"
+#include "ensemble.h"
+
+namespace cbc {
+
+template <int KB>
+__device__ __forceinline__ void ens_store_dense(const EnsLayout& E, const LaneState& S, const Geo& g, int s,
+                                                long long boff, int slot) {
+  if (g.li == 0) E.dense_time[(long long)slot * E.ns + s] = S.t;
+  double* d = E.dense_state + ((long long)slot * E.nb + boff + g.li) * 4;
+  reinterpret_cast<double2*>(d)[0] = make_double2(S.y[0], S.y[1]);
+  reinterpret_cast<double2*>(d)[1] = make_double2(S.y[2], S.y[3]);
+}
+
+// Loads system s into this lane's slot (lane li of the group) and runs the
+// prologue.  Called only by lanes whose group claimed s.
+template <int KB>
+__device__ __forceinline__ void ens_load(const EnsLayout& E, const Params& P, const Geo& g, int s, LaneState& S,
+                                         MView& M, double* hc, long long& boff) {
+  boff = E.bubble_offset[s];
+  const long long b = boff + g.li;
+  const double2* st = reinterpret_cast<const double2*>(E.state + b * 4);
+  const double2 s01 = st[0], s23 = st[1];
+  S.y[0] = s01.x;
+  S.y[1] = s01.y;
+  S.y[2] = s23.x;
+  S.y[3] = s23.y;
+  const double* up = E.unit_params + b * E.up_stride;
+#pragma unroll
+  for (int p = 0; p < 13; ++p) S.up[p] = up[p];
+  S.c73 = S.up[7] * (1.0 / 3.0);
+  S.c47 = S.up[4] * S.up[7];
+  const double* sp = E.system_params + (long long)s * E.sp_stride;
+  S.sp0 = sp[0];
+  S.sp3 = sp[3];
+  S.t = E.t[s];
+  S.t_end = E.t_end[s];
+  S.t_begin = E.t_begin[s];
+  S.h = E.h[s];
+  S.idx = (P.ndo > 0) ? E.dense_index[s] : 0;
+  const double prev = (P.ndo > 0 && S.idx > 0) ? E.dense_time[(long long)(S.idx - 1) * E.ns + s] : 0.0;
+  prologue(S, P, E.event[s], prev, E.status[s]);
+  M.m = E.coupling + E.coupling_offset[s] + g.li;
+  M.sc = (long long)g.K * g.K;
+  M.sj = g.K;
+  if (g.li == 0) store_harmonics(hc, g, sp[1], sp[2], sp[4], E.control_params + (long long)s * E.cp_stride, P.nk, 1);
+}
+
+template <int KB>
+__device__ __forceinline__ void ens_writeback(const EnsLayout& E, const Params& P, const Geo& g, int s,
+                                              long long boff, LaneState& S) {
+  double2* st = reinterpret_cast<double2*>(E.state + (boff + g.li) * 4);
+  st[0] = make_double2(S.y[0], S.y[1]);
+  st[1] = make_double2(S.y[2], S.y[3]);
+  if (g.li == 0) {
+    E.t[s] = S.t;
+    E.h[s] = S.h;
+    E.event[s] = S.g_old;
+    E.status[s] = S.status;
+    if (P.ndo > 0) E.dense_index[s] = S.idx;
+    if (E.steps) E.steps[s] += S.steps;
+    if (E.rejected) E.rejected[s] += S.rejected;
+    if (E.conv_ok) E.conv_ok[s] += S.conv_ok;
+    if (E.conv_fail) E.conv_fail[s] += S.conv_fail;
+    if (E.lin_iters) E.lin_iters[s] += S.lin_iters;
+  }
+}
+
+// Persistent worker: warps claim systems of bucket [begin, end) of the work
+// list until it is empty.  All systems of a bucket have the same K (<= KB).
+template <int KB>
+__global__ void __launch_bounds__(128) ensemble_kernel(EnsLayout E, Params P, const int* __restrict__ order,
+                                                       int begin, int end, int K, int* head,
+                                                       long long max_steps) {
+  extern __shared__ double smem[];
+  const Geo g = make_geo(K);
+  double* hc = smem + (threadIdx.x >> 5) * (HC_PER_K * P.nk * (32 / K));
+  const int lane = threadIdx.x & 31;
+  const bool leader = g.valid && g.li == 0;
+
+  LaneState S;
+  MView M;
+  M.m = E.coupling;
+  M.sc = M.sj = 0;
+  S.active = false;
+  S.status = ST_ACTIVE;
+  S.steps = 0;
+  int sys = -1;           // system in this lane's slot (-1: none)
+  long long boff = 0;
+  bool drained = false;   // work list exhausted for this warp (warp-uniform)
+
+  while (true) {
+    // ---- retire finished systems and refill empty slots (warp-uniform) ----
+    const bool retire = g.valid && sys >= 0 && !S.active;
+    if (__any_sync(FULL, retire)) {
+      if (retire) ens_writeback<KB>(E, P, g, sys, boff, S);
+      if (retire) sys = -1;
+    }
+    const bool want = leader && sys < 0 && !drained;
+    const unsigned wmask = __ballot_sync(FULL, want);
+    if (wmask) {
+      int base_idx = 0;
+      if (lane == 0) base_idx = atomicAdd(head, __popc(wmask));
+      base_idx = __shfl_sync(FULL, base_idx, 0);
+      int claim = -1;
+      if (want) {
+        const int idx = begin + base_idx + __popc(wmask & ((1u << lane) - 1u));
+        claim = (idx < end) ? order[idx] : -1;
+      }
+      if (__any_sync(FULL, want && claim < 0)) drained = true;
+      // hand the claimed system id to every lane of the group
+      const int got = __shfl_sync(FULL, claim, g.base);
+      const bool fresh = g.valid && sys < 0 && got >= 0 && __shfl_sync(FULL, (int)want, g.base);
+      if (fresh) {
+        sys = got;
+        ens_load<KB>(E, P, g, sys, S, M, hc, boff);
+      }
+      __syncwarp();
+      // first dense sample and initial event value for the fresh systems
+      if (fresh && S.active && P.ndo > 0) {
+        bool stq;
+        if (P.dense_mode == 0) stq = (S.idx < P.ndo) && (S.dnext <= S.t);
+        else stq = (S.idx < P.ndo) && (S.t >= grid_time(S, S.idx, P.ndo));
+        if (stq) {
+          ens_store_dense<KB>(E, S, g, sys, boff, S.idx);
+          S.idx += 1;
+          if (P.dense_mode == 0) {
+            const double nx = S.t + S.ddt;
+            S.dnext = nx < S.t_end ? nx : S.t_end;
+          }
+        }
+      }
+      const double g0 = group_event<KB>(S.y, S.up[12], g, P.col);
+      if (fresh && S.active) S.g_old = g0;
+      // systems that arrive already finished go straight back out
+      continue;
+    }
+    if (!__any_sync(FULL, S.active)) {
+      if (!__any_sync(FULL, sys >= 0)) break;  // nothing left in any slot
+      continue;
+    }
+    // ---- one Cash-Karp step for every active slot ----
+    const bool stq = step<KB>(g, P, hc, M, S);
+    if (stq) ens_store_dense<KB>(E, S, g, sys, boff, S.idx);
+    after_store(S, P, stq);
+    if (S.active && S.steps >= max_steps) {
+      S.status = ST_MAX_STEPS;
+      S.active = false;
+    }
+  }
+}
+
+template <int KB>
+cudaError_t launch_ensemble(const EnsLayout& E, const Params& P, const int* order, int begin, int end, int K,
+                            int* head, long long max_steps, int blocks, int threads, cudaStream_t stream) {
+  const size_t shmem = sizeof(double) * (size_t)(HC_PER_K * P.nk * (32 / K)) * (threads / 32);
+  ensemble_kernel<KB><<<blocks, threads, shmem, stream>>>(E, P, order, begin, end, K, head, max_steps);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ensemble_bucket(const EnsLayout& E, const Params& P, const int* order, int begin, int end,
+                                   int K, int* head, long long max_steps, int blocks, int threads,
+                                   cudaStream_t stream) {
+  switch (kb_for(K)) {
+    case 2: return launch_ensemble<2>(E, P, order, begin, end, K, head, max_steps, blocks, threads, stream);
+    case 4: return launch_ensemble<4>(E, P, order, begin, end, K, head, max_steps, blocks, threads, stream);
+    case 8: return launch_ensemble<8>(E, P, order, begin, end, K, head, max_steps, blocks, threads, stream);
+    case 16: return launch_ensemble<16>(E, P, order, begin, end, K, head, max_steps, blocks, threads, stream);
+    default: return launch_ensemble<32>(E, P, order, begin, end, K, head, max_steps, blocks, threads, stream);
+  }
+}
+
+int resident_blocks(int K, int nk, int threads) {
+  const size_t shmem = sizeof(double) * (size_t)(HC_PER_K * nk * (32 / K)) * (threads / 32);
+  int n = 0;
+  cudaError_t e;
+  switch (kb_for(K)) {
+    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<2>, threads, shmem); break;
+    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<4>, threads, shmem); break;
+    case 8: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<8>, threads, shmem); break;
+    case 16: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<16>, threads, shmem); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<32>, threads, shmem); break;
+  }
+  return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+}  // namespace cbc

@@ -1,0 +1,150 @@
+"""Generate golden vectors by running the REFERENCE numba integrator.
+
+Runs kalmi901/coupled-bubble-control's own CKM1D model and its default numba
+backend (``CKM1D(...).solve()`` -> ``backends/numba/rkck45_coupled_numba_solver.py``
+-> ``rkck45_coupled_numba_stepper.make_kernel``) under numba's CUDA simulator
+(NUMBA_ENABLE_CUDASIM=1) on the CPU of the build container, and stores the
+initial host buffers together with the reference's final buffers in
+``golden_ref_numba.npz``.  The reference tree is read from REFERENCE_ROOT
+(default /root/reference); it is not needed anywhere else.
+
+The simulator lacks a few features the reference relies on; these shims are
+applied before importing it and change no arithmetic:
+  * stub modules for cupy and matplotlib (imported but unused on this path);
+  * ``numba.cuda.cudadrv.devicearray.DeviceNDArray`` aliased to the
+    simulator's array type; ``cuda.default_stream`` returns stream 0;
+  * jit keyword arguments the simulator does not know are dropped;
+  * ``cuda.shfl_sync``/``cuda.activemask`` implemented with a block barrier
+    exchange.  This is exact when every thread of the block takes part, so the
+    cases use one system per block and K a power of two (TILE == UPS);
+  * the device helper ``sign(x) = (x > 0) - (x < 0)`` is evaluated on Python
+    ints (numpy booleans cannot be subtracted in simulator mode).
+Runtime is roughly a minute per case; the cases are tiny on purpose.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import threading
+import types
+
+os.environ["NUMBA_ENABLE_CUDASIM"] = "1"
+
+import numpy as np  # noqa: E402
+
+REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def install_shims():
+    for name in ("cupy", "matplotlib", "matplotlib.pyplot"):
+        m = types.ModuleType(name)
+        m.ndarray = type("ndarray", (), {})
+        sys.modules[name] = m
+    sys.modules["matplotlib"].pyplot = sys.modules["matplotlib.pyplot"]
+    from numba import cuda
+    from numba.cuda.simulator.cudadrv import devicearray as simda
+    da = types.ModuleType("numba.cuda.cudadrv.devicearray")
+    da.DeviceNDArray = simda.FakeCUDAArray
+    sys.modules["numba.cuda.cudadrv.devicearray"] = da
+    cuda.default_stream = lambda: 0
+
+    import numba.cuda.simulator.api as simapi
+    import numba.cuda.simulator.kernelapi as ka
+    orig_jit = simapi.jit
+
+    def jit(func_or_sig=None, **kw):
+        keep = {k: v for k, v in kw.items() if k in ("device", "debug", "argtypes", "inline", "restype",
+                                                       "fastmath", "link", "opt", "cache")}
+
+        def wrap(fn):
+            if getattr(fn, "__name__", "") == "sign":
+                def sign(x):
+                    return int(x > 0) - int(x < 0)
+                fn = sign
+            return orig_jit(**keep)(fn) if keep else orig_jit(fn)
+        if callable(func_or_sig):
+            return wrap(func_or_sig)
+        return wrap
+
+    cuda.jit = jit
+    simapi.jit = jit
+
+    def activemask(self):
+        return 0xFFFFFFFF
+
+    def shfl_sync(self, mask, val, src):
+        th = threading.current_thread()
+        mgr = th._manager
+        box = mgr.__dict__.setdefault("_shfl_box", {})
+        box[th.thread_id] = val
+        th.syncthreads()
+        out = box.get(int(src), val)
+        th.syncthreads()
+        return out
+
+    ka.FakeCUDAModule.activemask = activemask
+    ka.FakeCUDAModule.shfl_sync = shfl_sync
+
+
+# Small cases: (name, K, ac, nk, R0 um (K), PA bar (nk), FR kHz (nk), PS (units of pi), X0, t_end)
+CASES = [
+    ("k2_swa", 2, "SW_A", 2, [5.0, 3.0], [1.2, 0.4], [25.0, 50.0], [0.3, 1.1], [-0.05, 0.05], 0.004),
+    ("k2_swn", 2, "SW_N", 2, [6.0, 5.0], [0.5, 0.3], [25.0, 50.0], [0.0, 0.0], [-0.05, 0.05], 0.004),
+    ("k2_const", 2, "CONST", 1, [7.0, 5.0], [-1.2156], [20.0], [0.0], [0.0, 200e-6 / (1497.0 / 20e3)], 0.004),
+    ("k4_swa", 4, "SW_A", 2, [4.0, 6.0, 3.0, 5.0], [0.9, 0.7], [25.0, 50.0], [1.5, 0.2],
+     [-0.2, -0.1, 0.05, 0.2], 0.002),
+    ("k1_swa", 1, "SW_A", 2, [5.5], [1.4, 0.6], [25.0, 50.0], [0.1, 0.9], [0.1], 0.004),
+]
+
+
+def run_case(case, water):
+    from coupledbubble_control.models import CKM1D, MaterialProperties
+    from coupledbubble_control.backends import BackendName, KernelVariant
+    name, K, ac, nk, R0, PA, FR, PS, X0, t_end = case
+    ns = 1
+    mp = MaterialProperties()
+    if water:
+        for k, v in dict(RHO=998.0, CL=1497.0, ST=0.0728, VIS=1e-3, P0=1.0e5, PV=2330.0, PE=1.4).items():
+            setattr(mp, k, v)
+    model = CKM1D(num_systems=ns, systems_per_block=1, units_per_system=K,
+                  R0=np.array([R0], dtype=np.float64), PA=np.array(PA, dtype=np.float64)[:, None],
+                  FR=np.array(FR, dtype=np.float64)[:, None], PS=np.array(PS, dtype=np.float64)[:, None],
+                  REF_FREQ=FR[0], num_components=nk, acoustic_field=ac, mat_props=mp,
+                  backend=BackendName.NUMBA, variant=KernelVariant.SHARED, num_stored_points=0)
+    hb = model.runtime.host_buffers
+    hb.state.time_end[:] = t_end
+    hb.state.actual_state[1, :, :K] = np.array(X0)
+    init = {}
+    for grp in (hb.state, hb.params, hb.dense, hb.status):
+        for k in grp.__dataclass_fields__:
+            init[k] = np.array(getattr(grp, k), copy=True)
+    model.solve(max_steps=1_000_000, kernel_steps=1_000_000, sync_to_host=True)
+    final = {}
+    db = model.runtime.device_buffers
+    for grp_name in ("state", "status"):
+        grp = getattr(db, grp_name)
+        for k in grp.__dataclass_fields__:
+            final[k] = np.array(grp.__getattribute__(k).copy_to_host(), copy=True)
+    return init, final, dict(name=name, K=K, ac=ac, nk=nk)
+
+
+def main():
+    install_shims()
+    sys.path.insert(0, REF)
+    out = {}
+    for case in CASES:
+        print("running", case[0], flush=True)
+        init, final, meta = run_case(case, water=True)
+        for k, v in init.items():
+            out[f"{meta['name']}/init/{k}"] = v
+        for k, v in final.items():
+            out[f"{meta['name']}/final/{k}"] = v
+        out[f"{meta['name']}/meta"] = np.array([meta["K"], meta["nk"], ["CONST", "SW_N", "SW_A"].index(meta["ac"])])
+        print("  t", final["actual_time"], "R", final["actual_state"][0, 0, :meta["K"]], flush=True)
+    np.savez_compressed(os.path.join(HERE, "golden_ref_numba.npz"), **out)
+    print("wrote", os.path.join(HERE, "golden_ref_numba.npz"))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,69 @@
+"""GPU parity of the reference-layout solver against the CPU oracle.
+
+The CUDA kernels and the oracle perform the same IEEE operations in the same
+order (explicit fma, cbc_math elementary functions), so every output buffer
+must match bit for bit: states, times, step sizes, event values, statuses,
+dense output and counters.  Cases cover bubble counts 1..32, the three
+acoustic field types, both dense-output modes, both launch modes and
+different relaunch chunk sizes.
+"""
+import numpy as np
+import pytest
+
+from cbc_b200 import scenes
+from cbc_b200.models import SolverSpec
+
+from _parity import assert_bit_exact, run_pair
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("K", [1, 2, 3, 4, 5, 8])
+def test_bit_exact_small_k(cuda, K):
+    sc = scenes.uniform(K, ns=48, periods=0.5, seed=10 + K, samples_per_period=16)
+    gpu, ref = run_pair(sc)
+    assert_bit_exact(gpu, ref)
+    assert np.all(gpu["status_flags"] != 0)
+
+
+@pytest.mark.parametrize("K", [16, 32])
+def test_bit_exact_large_k(cuda, K):
+    sc = scenes.uniform(K, ns=6, periods=0.05, seed=20 + K, pa_hi=1.2, x_range=(-0.5, 0.5))
+    gpu, ref = run_pair(sc)
+    assert_bit_exact(gpu, ref)
+
+
+@pytest.mark.parametrize("ac", ["CONST", "SW_N", "SW_A"])
+def test_field_types(cuda, ac):
+    sc = scenes.uniform(2, ns=40, periods=0.5, seed=3, ac=ac, samples_per_period=8)
+    gpu, ref = run_pair(sc)
+    assert_bit_exact(gpu, ref)
+
+
+def test_grid_dense_mode(cuda):
+    sc = scenes.uniform(3, ns=40, periods=1.0, seed=5, samples_per_period=32)
+    gpu, ref = run_pair(sc, solver_spec=SolverSpec(dense_mode="grid"))
+    assert_bit_exact(gpu, ref)
+    ok = gpu["status_flags"] == 1
+    # every successful system sampled the full grid exactly
+    ndo = sc.ndo
+    assert np.all(gpu["dense_index"][ok] == ndo)
+    grid = np.linspace(0.0, 1.0, ndo)
+    np.testing.assert_allclose(gpu["dense_time"][:, ok], np.repeat(grid[:, None], ok.sum(), 1), rtol=0,
+                               atol=1e-15)
+
+
+@pytest.mark.parametrize("kernel_steps,mode", [(7, "relaunch"), (2048, "single"), (100000, "relaunch")])
+def test_launch_chunking_is_transparent(cuda, kernel_steps, mode):
+    """Results do not depend on how the step budget is cut into launches."""
+    sc = scenes.uniform(2, ns=32, periods=0.3, seed=7, samples_per_period=20)
+    gpu, ref = run_pair(sc, kernel_steps=kernel_steps, launch_mode=mode, max_steps=100_000)
+    assert_bit_exact(gpu, ref)
+
+
+def test_budget_exhaustion_sets_max_steps(cuda):
+    sc = scenes.uniform(2, ns=16, periods=2.0, seed=8)
+    gpu, ref = run_pair(sc, max_steps=50, kernel_steps=16)
+    assert_bit_exact(gpu, ref)
+    assert np.all(np.isin(gpu["status_flags"], [-1, -2, -3, 1]))
+    assert np.any(gpu["status_flags"] == -1)
