@@ -1,0 +1,361 @@
+"""Benchmark of the CKM1D ensemble integrator on B200.
+
+Metric (system-periods/s at rtol = atol = 1e-9): one system-period is one
+coupled-bubble system advanced by one period of the 25 kHz reference drive.
+Workload at N=1: the mixed-K batched ensemble -- 65,536 systems, K in
+{2,3,4,6,8} (p .4/.2/.2/.1/.1), spans U[5,50] periods, water, dual-frequency
+standing wave (25 + 50 kHz), FP64, seeded synthetic inputs (no dataset exists).
+A step is one batched solve of the whole ensemble (one CUDA-graph launch of
+the persistent work-stealing kernels) starting from the same initial state.
+
+Also measured (once, outside the timed steps): the plain one-launch-per-K
+reference-layout path on the same ensemble (the reference's execution model:
+one (NS, K) kernel per K, relaunched every 2048 steps with a host check).
+
+Multi-GPU (torchrun): weak scaling, every rank solves its own 65,536-system
+ensemble (seed + rank); no collective on the data path, only the final
+max-time / sum-work reduction.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "coupled-bubble-control_b200"), ROOT):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "system-periods/s @rtol 1e-9, batched vs plain; p50/p99 env-step latency"
+UNIT = "system-periods/s"
+MAX_STEPS = 1_000_000
+
+
+def flop_count(K, steps, lin_iters):
+    """Algorithmic FP64 flops (add/mul = 1, fma = 2, div/sqrt/pow/sin/cos = 1):
+    per step 6 RHS of 130K + 35K^2 (uncoupled RHS + explicit coupling) plus
+    240K + 10 (stages, error norm, controller), plus 20K^2 + 12K per
+    Richardson sweep of the implicit coupling."""
+    K = np.asarray(K, dtype=np.float64)
+    steps = np.asarray(steps, dtype=np.float64)
+    lin = np.asarray(lin_iters, dtype=np.float64)
+    per_step = 6.0 * (130.0 * K + 35.0 * K ** 2) + 240.0 * K + 10.0
+    return float(np.sum(steps * per_step + lin * (20.0 * K ** 2 + 12.0 * K)))
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks/throttle reasons every 200 ms while active."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def job_totals(rank_ms: float, rank_work: float, dist=None, device=None):
+    """Whole-job figures: the slowest rank's time and the work of all ranks.
+    Every rank must call this (it is a collective when ``dist`` is given)."""
+    if dist is None:
+        return rank_ms, rank_work
+    import torch
+    t = torch.tensor([rank_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    w = torch.tensor([rank_work], dtype=torch.float64, device=device)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(w.item())
+
+
+def rank_seed(rank: int) -> int:
+    """Each replica integrates its own ensemble (weak scaling)."""
+    return 1 + rank
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_fp64_peak(dev) -> float:
+    """cuBLAS FP64 GEMM throughput (TFLOP/s), best of 5: the measured FP64
+    denominator of the roofline (the driver's peaks file covers HBM and bf16)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_baseline(scene, seconds_hint: float = 15.0, nthreads: int = 0):
+    """The CPU oracle (C++ restatement of the reference integrator, all host
+    cores) on a bounded stratified sample of the same workload."""
+    from cbc_b200 import scenes
+    from oracle import oracle
+    rng = np.random.default_rng(99)
+    n = 96
+    idx = np.sort(rng.choice(scene.ns, size=n, replace=False))
+    sub = scenes.subset(scene, idx)
+    cap = 2.0
+    sub.t_end = np.minimum(sub.t_end, cap)
+    total_adv = 0.0
+    t0 = time.perf_counter()
+    for k in np.unique(sub.K):
+        sel = np.nonzero(sub.K == k)[0]
+        m = scenes.build_model(scenes.subset(sub, sel), ndo=0)
+        buf = oracle.solve_model(m, max_steps=MAX_STEPS, kernel_steps=MAX_STEPS, nthreads=nthreads)
+        total_adv += float(np.sum(buf["actual_time"]))
+    dt = time.perf_counter() - t0
+    cores = nthreads if nthreads > 0 else (os.cpu_count() or 1)
+    return {"value": total_adv / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} systems drawn from the same mixed-K ensemble, spans capped at {cap} periods "
+                      f"({total_adv:.1f} system-periods in {dt:.1f} s), CPU oracle on {cores} threads"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from cbc_b200 import scenes
+    scene = scenes.mixed_k(ns=args.ns, seed=1)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(scene)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"mixed_k_{args.ns}", "sample": "bounded CPU sample"},
+            "cpu_baseline": {**r, "value": v},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def plain_per_k(scene, dev):
+    """The reference execution model on the same systems: one reference-layout
+    solve per K (cbc_solve, relaunch every 2048 steps with a host check)."""
+    import torch
+    from cbc_b200 import scenes
+    total = 0.0
+    adv = 0.0
+    for k in np.unique(scene.K):
+        sel = np.nonzero(scene.K == k)[0]
+        m = scenes.build_model(scenes.subset(scene, sel), ndo=0)
+        m._ensure_buffers()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m.solve(max_steps=MAX_STEPS, kernel_steps=2048)
+        torch.cuda.synchronize()
+        total += time.perf_counter() - t0
+        adv += float(m.runtime.device_buffers.state.actual_time.sum().item())
+    return adv / total, total
+
+
+def run_b200(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        pg = dist
+    from cbc_b200 import scenes, _lib
+    from cbc_b200.ensemble import Ensemble
+
+    scene = scenes.mixed_k(ns=args.ns, seed=rank_seed(rank))
+    ens = Ensemble.from_scene(scene, device=local)
+    ens.to_device()
+    plan = ens.plan(MAX_STEPS)
+    nbuckets = int(np.unique(scene.K).size)
+    # pristine device copy of the initial state for the per-step reset
+    pristine = {k: v.clone() for k, v in ens.dev.items()}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def reset():
+        for k in ("state", "t", "h", "event", "status", "steps", "rejected", "conv_ok", "conv_fail", "lin_iters"):
+            ens.dev[k].copy_(pristine[k])
+        flush.fill_(1.0)  # write 256 MiB > L2 between steps
+
+    for _ in range(args.warmup):
+        reset()
+        plan.launch()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for i in range(args.steps):
+            reset()
+            ev[i][0].record()
+            plan.launch()
+            ev[i][1].record()
+        t1.record()
+        torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    total_ms = t0.elapsed_time(t1)
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    res = ens.to_host()
+    adv = float(np.sum(res["t"] - ens.host["t"]))
+    flops = flop_count(res["K"], res["steps"], res["lin_iters"])
+    status = {int(k): int(v) for k, v in zip(*np.unique(res["status"], return_counts=True))}
+
+    total_ms_all, work_all = job_totals(total_ms, adv * args.steps, pg, dev)
+    value = work_all / (total_ms_all * 1e-3)
+
+    # end-to-end through the public API from host buffers (rank-local)
+    e2e = None
+    if args.e2e:
+        keys_in = ("state", "t", "h", "event", "status", "steps", "rejected", "conv_ok", "conv_fail", "lin_iters")
+        keys_out = ("state", "t", "h", "event", "status", "steps", "rejected", "conv_ok", "conv_fail", "lin_iters")
+        pin_in = {k: torch.from_numpy(np.ascontiguousarray(ens.host[k])).pin_memory() for k in keys_in}
+        pin_out = {k: torch.empty_like(ens.dev[k], device="cpu").pin_memory() for k in keys_out}
+        h2d = sum(v.numel() * v.element_size() for v in pin_in.values())
+        d2h = sum(v.numel() * v.element_size() for v in pin_out.values())
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            for k in keys_in:
+                ens.dev[k].copy_(pin_in[k], non_blocking=True)
+            flush.fill_(1.0)
+            plan.launch()
+            for k in keys_out:
+                pin_out[k].copy_(ens.dev[k], non_blocking=True)
+        b.record()
+        torch.cuda.synchronize()
+        e2e_ms = a.elapsed_time(b)
+        e2e = {"value": adv * args.steps / (e2e_ms * 1e-3) * (world if pg else 1), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    plain = None
+    if args.plain and rank == 0:
+        pv, ptime = plain_per_k(scene, dev)
+        plain = {"value": pv, "unit": UNIT, "seconds": ptime,
+                 "how": "reference-layout solve per K (relaunch every 2048 steps + host completion check)"}
+
+    if rank == 0:
+        peak = measured_fp64_peak(dev)
+        mean_ms = float(np.mean(kern_ms))
+        achieved = flops / (mean_ms * 1e-3) / 1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms_all / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"mixed_k_{args.ns}", "ns_per_gpu": args.ns, "K": [2, 3, 4, 6, 8],
+                       "K_weights": [0.4, 0.2, 0.2, 0.1, 0.1], "span_periods": [5, 50], "rtol": 1e-9,
+                       "atol": 1e-9, "max_steps": MAX_STEPS, "field": "SW_A 25+50 kHz",
+                       "l2": "256 MiB buffer written before every step", "parallelism": f"replicas{world}"},
+            "work": {"advanced_system_periods_per_step": adv, "nominal_system_periods": float(np.sum(scene.t_end)),
+                     "status_counts": status, "steps_per_solve": int(np.sum(res["steps"])),
+                     "richardson_sweeps_per_rhs": float(np.sum(res["lin_iters"]) / max(1, 6 * np.sum(res["steps"]))),
+                     "algorithmic_gflop_per_step": flops / 1e9},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": "algorithmic FP64 flops (transcendentals counted as 1) / graph time; "
+                                 "peak = cuBLAS FP64 GEMM measured in this run"},
+            "clocks": clk.summary(),
+            "gpu_launches": args.steps * nbuckets,
+        }
+        if plain:
+            line["plain"] = plain
+            line["batched_vs_plain"] = value / world / plain["value"]
+        if e2e:
+            line["e2e"] = e2e
+        if world == 1 and args.cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(scene)
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--ns", type=int, default=65536)
+    ap.add_argument("--no-plain", dest="plain", action="store_false")
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -46,6 +46,24 @@ class cbc_solve_stats(ctypes.Structure):
     _fields_ = [("launches", i32), ("active_left", i32), ("device_ms", f64)]
 
 
+class cbc_ensemble(ctypes.Structure):
+    _fields_ = [("ns", i32), ("up_stride", i32), ("sp_stride", i32), ("cp_stride", i32), ("nb", i64)] + \
+        [(n, P) for n in ("bubble_offset", "coupling_offset", "state", "unit_params", "system_params",
+                          "control_params", "coupling", "t", "t_end", "t_begin", "h", "event", "status",
+                          "dense_index", "dense_time", "dense_state", "steps", "rejected", "conv_ok",
+                          "conv_fail", "lin_iters")]
+
+
+class cbc_work(ctypes.Structure):
+    _fields_ = [("order", P), ("nbuckets", i32), ("bucket_K", P), ("bucket_begin", P), ("threads", P),
+                ("blocks_per_sm", P)]
+
+
+class cbc_env_io(ctypes.Structure):
+    _fields_ = [("actions", P), ("n_act", i32), ("act_stride", i32), ("act_scale", f64), ("obs", P),
+                ("failed", P), ("K", i32), ("pad", i32), ("t_span", f64), ("h0", f64)]
+
+
 class CBCError(RuntimeError):
     """A C-ABI call returned a negative code."""
 
@@ -93,7 +111,16 @@ def _declare_extra(L) -> None:
             f.argtypes = args
 
 
-EXTRA_SIGNATURES: list = []
+EXTRA_SIGNATURES: list = [
+    ("cbc_ensemble_solve", i32, [P, ctypes.POINTER(cbc_spec), ctypes.POINTER(cbc_ensemble),
+                                 ctypes.POINTER(cbc_work), i64, P]),
+    ("cbc_plan_create", i32, [P, ctypes.POINTER(cbc_spec), ctypes.POINTER(cbc_ensemble),
+                              ctypes.POINTER(cbc_work), i64, ctypes.POINTER(P)]),
+    ("cbc_env_plan_create", i32, [P, ctypes.POINTER(cbc_spec), ctypes.POINTER(cbc_ensemble),
+                                  ctypes.POINTER(cbc_work), i64, ctypes.POINTER(cbc_env_io), ctypes.POINTER(P)]),
+    ("cbc_plan_launch", i32, [P, P]),
+    ("cbc_plan_destroy", i32, [P]),
+]
 
 
 def check(rc: int, ctx: Optional[int] = None) -> None:

@@ -1,0 +1,228 @@
+// capi_ensemble.cu -- C ABI of the batched mixed-K form: direct solve and
+// CUDA-graph plans.  See ensemble.cu for the device side.
+#include <new>
+#include <vector>
+
+#include "cbc_internal.h"
+#include "ensemble.h"
+
+struct cbc_plan {
+  cbc_context* ctx = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int* d_head = nullptr;  // one work-list cursor per bucket
+  int nbuckets = 0;
+};
+
+namespace cbc {
+
+int32_t enqueue_env_begin(cbc_context* ctx, const cbc_ensemble* e, const cbc_env_io* io, cudaStream_t st);
+int32_t enqueue_env_end(cbc_context* ctx, const cbc_ensemble* e, const cbc_env_io* io, cudaStream_t st);
+
+static int32_t check_ensemble(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e, const cbc_work* w) {
+  if (!spec) return fail(ctx, CBC_E_INVALID, "spec is NULL");
+  if (spec->nk < 1 || spec->nk > NKMAX)
+    return fail(ctx, CBC_E_UNSUPPORTED, "nk = %d: 1..%d harmonic components supported", spec->nk, NKMAX);
+  if (spec->ac < 0 || spec->ac > 2) return fail(ctx, CBC_E_INVALID, "ac = %d out of range", spec->ac);
+  if (spec->ndo < 0 || spec->dense_mode < 0 || spec->dense_mode > 1 || spec->lin_max_iter < 0)
+    return fail(ctx, CBC_E_INVALID, "ndo, dense_mode or lin_max_iter out of range");
+  if (!(spec->min_step > 0.0) || !(spec->max_step >= spec->min_step) || !(spec->atol > 0.0))
+    return fail(ctx, CBC_E_INVALID, "need 0 < min_step <= max_step and atol > 0");
+  if (!e || !w) return fail(ctx, CBC_E_INVALID, "ensemble or work list is NULL");
+  if (e->ns < 1 || e->nb < 1) return fail(ctx, CBC_E_INVALID, "empty ensemble");
+  if (!e->bubble_offset || !e->coupling_offset || !e->state || !e->unit_params || !e->system_params ||
+      !e->control_params || !e->coupling || !e->t || !e->t_end || !e->t_begin || !e->h || !e->event || !e->status)
+    return fail(ctx, CBC_E_INVALID, "a required ensemble pointer is NULL");
+  if (spec->ndo > 0 && (!e->dense_index || !e->dense_time || !e->dense_state))
+    return fail(ctx, CBC_E_INVALID, "ndo > 0 needs dense_index, dense_time and dense_state");
+  if (e->up_stride < 13 || e->sp_stride < 5 || e->cp_stride < 4 * spec->nk)
+    return fail(ctx, CBC_E_INVALID, "parameter row strides too small (need >= 13, 5, 4 nk)");
+  if (((uintptr_t)e->state & 15) || (spec->ndo > 0 && ((uintptr_t)e->dense_state & 15)))
+    return fail(ctx, CBC_E_INVALID, "state and dense_state must be 16-byte aligned");
+  if (!w->order || w->nbuckets < 1 || w->nbuckets > CBC_MAX_BUCKETS || !w->bucket_K || !w->bucket_begin)
+    return fail(ctx, CBC_E_INVALID, "work list needs 1..%d buckets", CBC_MAX_BUCKETS);
+  for (int b = 0; b < w->nbuckets; ++b) {
+    const int K = w->bucket_K[b];
+    if (K < 1 || K > 32) return fail(ctx, CBC_E_UNSUPPORTED, "bucket %d: K = %d (1..32 supported)", b, K);
+    if (w->bucket_begin[b] < 0 || w->bucket_begin[b + 1] < w->bucket_begin[b])
+      return fail(ctx, CBC_E_INVALID, "bucket %d: bad range", b);
+    if (w->threads && (w->threads[b] < 32 || w->threads[b] > 128 || (w->threads[b] & 31)))
+      return fail(ctx, CBC_E_INVALID, "bucket %d: threads per block must be 32..128, a multiple of 32", b);
+  }
+  return CBC_OK;
+}
+
+static EnsLayout make_layout(const cbc_ensemble* e) {
+  EnsLayout E;
+  E.ns = e->ns;
+  E.nb = e->nb;
+  E.bubble_offset = (const long long*)e->bubble_offset;
+  E.coupling_offset = (const long long*)e->coupling_offset;
+  E.state = e->state;
+  E.unit_params = e->unit_params;
+  E.system_params = e->system_params;
+  E.control_params = e->control_params;
+  E.coupling = e->coupling;
+  E.t = e->t;
+  E.t_end = e->t_end;
+  E.t_begin = e->t_begin;
+  E.h = e->h;
+  E.event = e->event;
+  E.status = e->status;
+  E.dense_index = e->dense_index;
+  E.dense_time = e->dense_time;
+  E.dense_state = e->dense_state;
+  E.steps = e->steps;
+  E.rejected = e->rejected;
+  E.conv_ok = e->conv_ok;
+  E.conv_fail = e->conv_fail;
+  E.lin_iters = (long long*)e->lin_iters;
+  E.up_stride = e->up_stride;
+  E.sp_stride = e->sp_stride;
+  E.cp_stride = e->cp_stride;
+  return E;
+}
+
+// Persistent grid size per bucket: resident blocks per SM (occupancy, or the
+// work list's override if smaller) times the SM count, but never more warps
+// than the bucket has system slots to fill.  Computed before any capture.
+static std::vector<int> grid_sizes(cbc_context* ctx, const cbc_spec* spec, const cbc_work* w) {
+  std::vector<int> out(w->nbuckets, 0);
+  for (int b = 0; b < w->nbuckets; ++b) {
+    const int begin = w->bucket_begin[b], end = w->bucket_begin[b + 1];
+    if (end <= begin) continue;
+    const int K = w->bucket_K[b];
+    const int threads = w->threads ? w->threads[b] : 128;
+    const int per_sm = resident_blocks(K, spec->nk, threads);
+    int blocks = per_sm * ctx->sm_count;
+    if (w->blocks_per_sm && w->blocks_per_sm[b] > 0 && w->blocks_per_sm[b] < per_sm)
+      blocks = w->blocks_per_sm[b] * ctx->sm_count;
+    const long long warps_needed = ((long long)(end - begin) + (32 / K) - 1) / (32 / K);
+    const long long blocks_needed = (warps_needed * 32 + threads - 1) / threads;
+    if (blocks > blocks_needed) blocks = (int)blocks_needed;
+    out[b] = blocks;
+  }
+  return out;
+}
+
+// Enqueues the whole batched solve on `stream`: every bucket on its own
+// forked stream (ctx->side[b]), joined back into `stream`.
+static int32_t enqueue(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e, const cbc_work* w,
+                       const std::vector<int>& grids, int64_t max_steps, int* d_head, cudaStream_t stream) {
+  const EnsLayout E = make_layout(e);
+  const Params P = make_params(*spec);
+  CBC_CUDA_TRY(ctx, cudaMemsetAsync(d_head, 0, sizeof(int) * w->nbuckets, stream));
+  CBC_CUDA_TRY(ctx, cudaEventRecord(ctx->fork, stream));
+  int used = 0;
+  for (int b = 0; b < w->nbuckets; ++b) {
+    const int begin = w->bucket_begin[b], end = w->bucket_begin[b + 1];
+    if (end <= begin) continue;
+    const int K = w->bucket_K[b];
+    const int threads = w->threads ? w->threads[b] : 128;
+    const int blocks = grids[b];
+    cudaStream_t s = ctx->side[used % CBC_SIDE_STREAMS];
+    CBC_CUDA_TRY(ctx, cudaStreamWaitEvent(s, ctx->fork, 0));
+    CBC_CUDA_TRY(ctx, launch_ensemble_bucket(E, P, w->order, begin, end, K, d_head + b, max_steps, blocks,
+                                             threads, s));
+    CBC_CUDA_TRY(ctx, cudaEventRecord(ctx->join[used % CBC_SIDE_STREAMS], s));
+    CBC_CUDA_TRY(ctx, cudaStreamWaitEvent(stream, ctx->join[used % CBC_SIDE_STREAMS], 0));
+    ++used;
+  }
+  return CBC_OK;
+}
+
+}  // namespace cbc
+
+using namespace cbc;
+
+extern "C" {
+
+int32_t cbc_ensemble_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e, const cbc_work* w,
+                           int64_t max_steps, void* stream) {
+  if (!ctx) return fail(nullptr, CBC_E_INVALID, "context is NULL");
+  ctx->err.clear();
+  int32_t rc = check_ensemble(ctx, spec, e, w);
+  if (rc) return rc;
+  if (max_steps < 1) return fail(ctx, CBC_E_INVALID, "max_steps must be >= 1");
+  DeviceGuard dg(ctx->device);
+  const std::vector<int> grids = grid_sizes(ctx, spec, w);
+  return enqueue(ctx, spec, e, w, grids, max_steps, ctx->d_head, (cudaStream_t)stream);
+}
+
+int32_t cbc_plan_create(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e, const cbc_work* w,
+                        int64_t max_steps, cbc_plan** out) {
+  return cbc_env_plan_create(ctx, spec, e, w, max_steps, nullptr, out);
+}
+
+int32_t cbc_env_plan_create(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e, const cbc_work* w,
+                            int64_t max_steps, const cbc_env_io* io, cbc_plan** out) {
+  if (!ctx) return fail(nullptr, CBC_E_INVALID, "context is NULL");
+  ctx->err.clear();
+  if (!out) return fail(ctx, CBC_E_INVALID, "out is NULL");
+  *out = nullptr;
+  int32_t rc = check_ensemble(ctx, spec, e, w);
+  if (rc) return rc;
+  if (max_steps < 1) return fail(ctx, CBC_E_INVALID, "max_steps must be >= 1");
+  if (io) {
+    if (!io->actions || !io->obs || io->n_act < 0 || io->n_act > e->cp_stride || io->act_stride < io->n_act ||
+        io->K < 1 || io->K > 32 || (long long)io->K * e->ns != e->nb || !(io->t_span > 0.0) || !(io->h0 > 0.0))
+      return fail(ctx, CBC_E_INVALID, "env io: need actions, obs, 0 <= n_act <= cp_stride, a uniform K with "
+                                      "ns * K == nb, t_span > 0 and h0 > 0");
+  }
+  DeviceGuard dg(ctx->device);
+  cbc_plan* p = new (std::nothrow) cbc_plan();
+  if (!p) return fail(ctx, CBC_E_NOMEM, "plan allocation failed");
+  p->ctx = ctx;
+  p->nbuckets = w->nbuckets;
+  cudaError_t ce = cudaMalloc(&p->d_head, sizeof(int) * CBC_MAX_BUCKETS);
+  if (ce != cudaSuccess) {
+    delete p;
+    return fail(ctx, CBC_E_CUDA, "cudaMalloc: %s", cudaGetErrorString(ce));
+  }
+  const std::vector<int> grids = grid_sizes(ctx, spec, w);
+  cudaStream_t cs = ctx->capture;
+  ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (ce != cudaSuccess) {
+    cbc_plan_destroy(p);
+    return fail(ctx, CBC_E_CUDA, "cudaStreamBeginCapture: %s", cudaGetErrorString(ce));
+  }
+  if (io) rc = enqueue_env_begin(ctx, e, io, cs);
+  if (rc == CBC_OK) rc = enqueue(ctx, spec, e, w, grids, max_steps, p->d_head, cs);
+  if (rc == CBC_OK && io) rc = enqueue_env_end(ctx, e, io, cs);
+  cudaGraph_t g = nullptr;
+  ce = cudaStreamEndCapture(cs, &g);
+  if (rc != CBC_OK || ce != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cbc_plan_destroy(p);
+    if (rc != CBC_OK) return rc;
+    return fail(ctx, CBC_E_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(ce));
+  }
+  p->graph = g;
+  ce = cudaGraphInstantiate(&p->exec, g, 0);
+  if (ce != cudaSuccess) {
+    cbc_plan_destroy(p);
+    return fail(ctx, CBC_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(ce));
+  }
+  *out = p;
+  return CBC_OK;
+}
+
+int32_t cbc_plan_launch(cbc_plan* p, void* stream) {
+  if (!p) return fail(nullptr, CBC_E_INVALID, "plan is NULL");
+  p->ctx->err.clear();
+  DeviceGuard dg(p->ctx->device);
+  CBC_CUDA_TRY(p->ctx, cudaGraphLaunch(p->exec, (cudaStream_t)stream));
+  return CBC_OK;
+}
+
+int32_t cbc_plan_destroy(cbc_plan* p) {
+  if (!p) return CBC_OK;
+  DeviceGuard dg(p->ctx->device);
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->d_head) cudaFree(p->d_head);
+  delete p;
+  return CBC_OK;
+}
+
+}  // extern "C"

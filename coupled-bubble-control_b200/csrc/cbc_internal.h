@@ -13,16 +13,35 @@
 #include "../../include/cbc_b200.h"
 #include "ckm1d_core.cuh"
 
+#define CBC_MAX_BUCKETS 64
+#define CBC_SIDE_STREAMS 8
+
 struct cbc_context {
   int device = 0;
   int sm_count = 0;
   int* d_counter = nullptr;       // device: systems still active after a launch
   int* h_counter = nullptr;       // pinned host mirror
+  int* d_head = nullptr;          // device: work-list cursors of cbc_ensemble_solve
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[CBC_SIDE_STREAMS] = {};
+  cudaStream_t side[CBC_SIDE_STREAMS] = {};
+  cudaStream_t capture = nullptr;  // stream used to capture plans into graphs
   std::string err;
 };
 
 namespace cbc {
+
+// Makes `device` current for the lifetime of the guard, restoring the
+// caller's device afterwards.
+struct DeviceGuard {
+  int prev = 0;
+  explicit DeviceGuard(int device) {
+    cudaGetDevice(&prev);
+    if (prev != device) cudaSetDevice(device);
+  }
+  ~DeviceGuard() { cudaSetDevice(prev); }
+};
 
 // Message store for failures that happen without a context.
 inline std::string& global_error() {

@@ -12,14 +12,24 @@
 // every lane of the group and stay identical because every lane computes them
 // from the same shuffled inputs.
 //
+// Canonical evaluation order (shared with oracle/ckm1d_oracle.cpp):
+//   * pair sums of bubble i run over the partners j = (i + d) mod K,
+//     d = 1 .. K-1 (every lane does useful work in every iteration; no
+//     masked diagonal term);
+//   * sums over the bubbles of a system (norms of the implicit-coupling
+//     iteration) are pairwise trees over the next power of two, zero padded;
+//   * min / all reductions are order independent.
 // Numerics: FP64 throughout, compiled with -fmad=false; every fused
-// multiply-add is an explicit fma().  Operation order matches
-// oracle/ckm1d_oracle.cpp line for line, and the elementary functions come
-// from cbc_math.h, so results equal the CPU oracle bit for bit.  The algorithm
+// multiply-add is an explicit fma() and the elementary functions come from
+// cbc_math.h, so results equal the CPU oracle bit for bit.  The algorithm
 // restates coupledbubble_control/backends/numba/sysmtem_definitions/ckm1d_def.py
 // (acoustic_field_1d :79-114, ode_fun :408-497, explicit_coupling :164-246,
 // mat_vec_product :250-299, implicit_coupling :303-404, event_fun :499-556) and
 // rkck45_coupled_numba_stepper.py (:362-677).
+//
+// Per-warp shared memory (WarpSmem): the group's harmonic constants, the
+// lane's 13 bubble constants (+2 derived) and the six stage derivatives.
+// Keeping these out of registers lets more warps stay resident.
 #pragma once
 
 #include <stdint.h>
@@ -30,6 +40,7 @@ namespace cbc {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int NKMAX = 4;                        // harmonic components supported
 constexpr int HC_PER_K = 7;                     // per-harmonic constants
+constexpr int NUPS = 15;                        // 13 bubble constants + up7/3 + up4*up7
 constexpr double TWO_PI = 6.283185307179586;    // 2.0 * np.pi
 
 // Cash-Karp tableau (stepper.py:15-24)
@@ -44,6 +55,21 @@ constexpr double C1 = 37.0 / 378.0, C3 = 250.0 / 621.0, C4 = 125.0 / 594.0, C6 =
 constexpr double CP1 = 2825.0 / 27648.0, CP3 = 18575.0 / 48384.0, CP4 = 13525.0 / 55296.0,
                  CP5 = 277.0 / 14336.0, CP6 = 1.0 / 4.0;
 constexpr double CE1 = C1 - CP1, CE3 = C3 - CP3, CE4 = C4 - CP4, CE5 = 0.0 - CP5, CE6 = C6 - CP6;
+
+// Stage tableau for the stage loop: row s (1..5) combines k_1..k_s.
+static __constant__ double kStageA[6] = {0.0, A2, A3, A4, A5, A6};
+static __constant__ double kStageB[6][5] = {{0, 0, 0, 0, 0},
+                                     {B21, 0, 0, 0, 0},
+                                     {B31, B32, 0, 0, 0},
+                                     {B41, B42, B43, 0, 0},
+                                     {B51, B52, B53, B54, 0},
+                                     {B61, B62, B63, B64, B65}};
+
+// Resident 128-thread blocks per SM the register allocation is tuned for, per
+// lanes-per-system instantiation (ptxas: KB=2 fits 128 registers and KB=4 168
+// without spills; KB=8 needs ~250; KB >= 16 keeps its pair arrays in local
+// memory either way).
+__host__ __device__ constexpr int min_blocks_for(int KB) { return KB <= 2 ? 4 : (KB <= 4 ? 3 : (KB <= 8 ? 2 : 1)); }
 
 // Per-system status codes (stepper.py:27-33).
 enum : int {
@@ -69,12 +95,14 @@ struct Geo {
   int grp;     // group index (clamped to a valid slot for idle lanes)
   int base;    // first lane of the group
   int li;      // bubble index of this lane
+  int lane;
   bool valid;  // lane belongs to a group
 };
 
 __device__ __forceinline__ Geo make_geo(int K) {
   Geo g;
   const int lane = threadIdx.x & 31;
+  g.lane = lane;
   g.K = K;
   g.G = 32 / K;
   const int grp = lane / K;
@@ -87,6 +115,33 @@ __device__ __forceinline__ Geo make_geo(int K) {
 
 __device__ __forceinline__ double shfl(double v, int src) { return __shfl_sync(FULL, v, src); }
 
+// Source lane of partner d (1 <= d < K) of this lane: bubble (li + d) mod K.
+__device__ __forceinline__ int partner_lane(const Geo& g, int d) {
+  int j = g.li + d;
+  if (j >= g.K) j -= g.K;
+  return g.base + j;
+}
+
+// Per-warp shared-memory carve-up, in doubles.
+struct WarpSmem {
+  double* hc;   // [7 nk][G]   harmonic constants of each group (component-major)
+  double* up;   // [15][32]    bubble constants, lane-private columns
+  double* ks;   // [6][4][32]  stage derivatives, lane-private columns
+};
+
+__host__ __device__ inline int smem_doubles_per_warp(int K, int nk) {
+  return HC_PER_K * nk * (32 / K) + NUPS * 32 + 24 * 32;
+}
+
+__device__ __forceinline__ WarpSmem warp_smem(double* base, int K, int nk) {
+  WarpSmem w;
+  double* p = base + (threadIdx.x >> 5) * smem_doubles_per_warp(K, nk);
+  w.hc = p;
+  w.up = p + HC_PER_K * nk * (32 / K);
+  w.ks = w.up + NUPS * 32;
+  return w;
+}
+
 // Coupling matrices of this lane's system: M(c, j, i=this lane) = m[c*sc + j*sj]
 struct MView {
   const double* __restrict__ m;  // points at M(0, 0, i)
@@ -96,8 +151,6 @@ struct MView {
 // Per-lane integrator state (bubble + copies of the system scalars).
 struct LaneState {
   double y[4];                 // R, X, U, V
-  double up[13];
-  double c73, c47;             // up7/3, up4*up7
   double sp0, sp3;             // 3 gamma, c
   double t, t_end, t_begin, h, g_old;
   double dnext, ddt;           // dense schedule (next sample time, spacing)
@@ -108,13 +161,24 @@ struct LaneState {
   long long lin_iters;
 };
 
-// Per-system harmonic constants in shared memory, component-major so that
-// the groups of a warp hit distinct banks: hc[(7k + c) * G + grp].
+// Writes this lane's bubble constants (13 from the caller, 2 derived).
+__device__ __forceinline__ void store_bubble_consts(const WarpSmem& w, const Geo& g, const double* up13,
+                                                    long long stride) {
+  double* u = w.up + g.lane;
+#pragma unroll
+  for (int p = 0; p < 13; ++p) u[p * 32] = up13[p * stride];
+  u[13 * 32] = u[7 * 32] * (1.0 / 3.0);
+  u[14 * 32] = u[4 * 32] * u[7 * 32];
+}
+
+__device__ __forceinline__ double upv(const WarpSmem& w, const Geo& g, int p) { return w.up[p * 32 + g.lane]; }
+
+// Per-system harmonic constants, component-major: hc[(7k + c) * G + grp].
 //   c = 0 w0*omega, 1 phase, 2 l0*wave, 3 PA, 4 PA*omega, 5 PA*wave, 6 PA*u0
 // Written by lane 0 of the group from system parameters sp1 = 1/omega_ref,
 // sp2 = lambda_ref/2pi, sp4 = 1/(rho c) and the control parameters
 // cp[m * cp_stride], m = 0..4nk-1 (PA, omega, phase, wave number).
-__device__ __forceinline__ void store_harmonics(double* hc, const Geo& g, double sp1, double sp2,
+__device__ __forceinline__ void store_harmonics(const WarpSmem& w, const Geo& g, double sp1, double sp2,
                                                 double sp4, const double* cp, int nk,
                                                 long long cp_stride) {
   // acoustic_field_1d (ckm1d_def.py:95-97): w0 = 2pi sp[1], l0 = 2pi sp[2], u0 = sp[4]
@@ -124,7 +188,7 @@ __device__ __forceinline__ void store_harmonics(double* hc, const Geo& g, double
   for (int k = 0; k < nk; ++k) {
     const double amps = cp[k * cp_stride], omega = cp[(nk + k) * cp_stride],
                  phase = cp[(2 * nk + k) * cp_stride], wave = cp[(3 * nk + k) * cp_stride];
-    double* h = hc + (HC_PER_K * k) * g.G + g.grp;
+    double* h = w.hc + (HC_PER_K * k) * g.G + g.grp;
     h[0 * g.G] = w0 * omega;
     h[1 * g.G] = phase;
     h[2 * g.G] = l0 * wave;
@@ -135,32 +199,42 @@ __device__ __forceinline__ void store_harmonics(double* hc, const Geo& g, double
   }
 }
 
-__device__ __forceinline__ double hcv(const double* hc, const Geo& g, int k, int c) {
-  return hc[(HC_PER_K * k + c) * g.G + g.grp];
+__device__ __forceinline__ double hcv(const WarpSmem& w, const Geo& g, int k, int c) {
+  return w.hc[(HC_PER_K * k + c) * g.G + g.grp];
 }
 
-// Sum of v over the group, ascending bubble index (fixed order).
+// Pairwise-tree sum of v over the group (next power of two, zero padded):
+// every lane ends with ((v0 + v1) + (v2 + v3)) + ...  At level w each lane
+// holds the sum of its aligned block of w bubbles; the partner block starts
+// at q = (li ^ w) & ~(w - 1) and is read from its first lane (which exists
+// unless the whole block is padding, then it contributes +0.0).  IEEE
+// addition is commutative, so both blocks of a pair compute the same sum.
 template <int KB>
 __device__ __forceinline__ double group_sum(double v, const Geo& g) {
-  double s = 0.0;
 #pragma unroll
-  for (int j = 0; j < KB; ++j)
-    if (j < g.K) s = s + shfl(v, g.base + j);
-  return s;
+  for (int w = 1; w < KB; w <<= 1) {
+    if (w < g.K) {
+      const int q = (g.li ^ w) & ~(w - 1);
+      double x = shfl(v, g.base + (q < g.K ? q : g.li));
+      if (q >= g.K) x = 0.0;
+      v = v + x;
+    }
+  }
+  return v;
 }
 
-// Minimum of v over the group, starting from 1e30; NaN entries never win
-// (same as the oracle's sequential "if (v < m) m = v" scan).
+// Minimum over the group (order independent; NaN never wins).
 template <int KB>
 __device__ __forceinline__ double group_min(double v, const Geo& g) {
-  double m = 1.0e30;
 #pragma unroll
-  for (int j = 0; j < KB; ++j)
-    if (j < g.K) {
-      const double x = shfl(v, g.base + j);
-      if (x < m) m = x;
+  for (int w = 1; w < KB; w <<= 1) {
+    if (w < g.K) {
+      const int q = (g.li ^ w) & ~(w - 1);
+      const double x = shfl(v, g.base + (q < g.K ? q : g.li));
+      if (q < g.K && x < v) v = x;
     }
-  return m;
+  }
+  return v;
 }
 
 // AND of a per-lane predicate over the group.
@@ -171,7 +245,8 @@ __device__ __forceinline__ bool group_all(bool p, const Geo& g) {
 }
 
 // event_fun (ckm1d_def.py:499-556): min over neighbours of
-// |x_i - x_{i+1}| - (R_i R0_i + R_{i+1} R0_{i+1}) / lambda * (1 + threshold).
+// |x_i - x_{i+1}| - (R_i R0_i + R_{i+1} R0_{i+1}) / lambda * (1 + threshold),
+// 1e30 for a single bubble.
 template <int KB>
 __device__ __forceinline__ double group_event(const double y[4], double up12, const Geo& g, double col) {
   const double ri = y[0] * up12;
@@ -179,22 +254,17 @@ __device__ __forceinline__ double group_event(const double y[4], double up12, co
   const double xj = __shfl_down_sync(FULL, y[1], 1);
   double gap = 1e30;
   if (g.li + 1 < g.K) gap = fabs(y[1] - xj) - (ri + rj) * col;
-  // sequential min with initial 1e30 (NaN never wins)
-  double m = 1e30;
-#pragma unroll
-  for (int j = 0; j < KB; ++j)
-    if (j < g.K) {
-      const double x = shfl(gap, g.base + j);
-      if (x < m) m = x;
-    }
-  return m;
+  // a sequential "if (gap < m) m = gap" scan from 1e30 ignores NaN and values
+  // >= 1e30; clamp first so that the tree reduction agrees with it
+  if (!(gap < 1e30)) gap = 1e30;
+  return group_min<KB>(gap, g);
 }
 
 // RHS of the whole system, evaluated by its K lanes: dy of this lane's bubble.
 // Returns via conv/iters the outcome of the implicit-coupling iteration.
 template <int KB>
-__device__ __forceinline__ void rhs(const Geo& g, const Params& P, const double* hc, const MView& M,
-                                    const LaneState& S, bool on, double t, const double y[4],
+__device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSmem& W, const MView& M,
+                                    double sp0, double sp3, bool on, double t, const double y[4],
                                     double dy[4], bool& conv, int& iters) {
   const int K = g.K;
   const int li = g.li;
@@ -205,7 +275,7 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const double*
   if (P.nk <= K) {
     const int k = li < P.nk ? li : 0;
     double s_, c_;
-    cbcm::sincos(fma(hcv(hc, g, k, 0), t, hcv(hc, g, k, 1)), &s_, &c_);
+    cbcm::sincos(fma(hcv(W, g, k, 0), t, hcv(W, g, k, 1)), &s_, &c_);
 #pragma unroll
     for (int kk = 0; kk < NKMAX; ++kk)
       if (kk < P.nk) {
@@ -215,25 +285,24 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const double*
   } else {
 #pragma unroll
     for (int kk = 0; kk < NKMAX; ++kk)
-      if (kk < P.nk) cbcm::sincos(fma(hcv(hc, g, kk, 0), t, hcv(hc, g, kk, 1)), &st[kk], &ct[kk]);
+      if (kk < P.nk) cbcm::sincos(fma(hcv(W, g, kk, 0), t, hcv(W, g, kk, 1)), &st[kk], &ct[kk]);
   }
 
   // ---- uncoupled Keller--Miksis + translation (ckm1d_def.py:418-447) ----
-  const double* up = S.up;
   const double rx0 = 1.0 / x0;
-  const double p = cbcm::pow_pos(rx0, S.sp0);
+  const double p = cbcm::pow_pos(rx0, sp0);
   double pa = 0.0, pt = 0.0, px = 0.0, ux = 0.0;
 #pragma unroll
   for (int k = 0; k < NKMAX; ++k) {
     if (k < P.nk) {
-      const double a = hcv(hc, g, k, 3), aw = hcv(hc, g, k, 4);
+      const double a = hcv(W, g, k, 3), aw = hcv(W, g, k, 4);
       if (P.ac == 0) {  // CONST
         pa = fma(a, st[k], pa);
         pt = fma(aw, ct[k], pt);
       } else {
         double sx, cx;
-        cbcm::sincos(fma(hcv(hc, g, k, 2), x1, hcv(hc, g, k, 1)), &sx, &cx);
-        const double awv = hcv(hc, g, k, 5), au = hcv(hc, g, k, 6);
+        cbcm::sincos(fma(hcv(W, g, k, 2), x1, hcv(W, g, k, 1)), &sx, &cx);
+        const double awv = hcv(W, g, k, 5), au = hcv(W, g, k, 6);
         if (P.ac == 1) {  // SW_N
           pa = fma(a * sx, st[k], pa);
           pt = fma(aw * sx, ct[k], pt);
@@ -248,39 +317,41 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const double*
       }
     }
   }
-  const double q = fma(up[7], x2, 1.0);
-  double N = fma(up[1], x2, up[0]) * p;
-  N = fma(-up[2], q, N);
-  N = fma(-up[3], rx0, N);
-  N = fma(-(up[4] * x2), rx0, N);
-  const double w = fma(-S.c73, x2, 1.0);
+  const double u7 = upv(W, g, 7);
+  const double q = fma(u7, x2, 1.0);
+  double N = fma(upv(W, g, 1), x2, upv(W, g, 0)) * p;
+  N = fma(-upv(W, g, 2), q, N);
+  N = fma(-upv(W, g, 3), rx0, N);
+  N = fma(-(upv(W, g, 4) * x2), rx0, N);
+  const double w = fma(-upv(W, g, 13), x2, 1.0);
   N = fma((-1.5 * w) * x2, x2, N);
-  N = fma(-(q * up[5]), pa, N);
-  N = fma(-(up[6] * pt), x0, N);
-  N = fma(up[8] * x3, x3, N);
-  const double D = fma(-(up[7] * x0), x2, x0) + S.c47;
+  N = fma(-(q * upv(W, g, 5)), pa, N);
+  N = fma(-(upv(W, g, 6) * pt), x0, N);
+  N = fma(upv(W, g, 8) * x3, x3, N);
+  const double D = fma(-(u7 * x0), x2, x0) + upv(W, g, 14);
   const double rD = 1.0 / D;
   const double x02 = x0 * x0;
   const double x03 = x02 * x0;
-  const double Fb1 = -(up[10] * x03) * px;
-  const double Fd = -(up[11] * x0) * fma(x3, S.sp3, -ux);
+  const double Fb1 = -(upv(W, g, 10) * x03) * px;
+  const double Fd = -(upv(W, g, 11) * x0) * fma(x3, sp3, -ux);
   const double rx03 = (rx0 * rx0) * rx0;
   double b0 = N * rD;
-  double b1 = fma((3.0 * (Fb1 + Fd)) * up[9], rx03, -(((3.0 * x2) * rx0) * x3));
+  double b1 = fma((3.0 * (Fb1 + Fd)) * upv(W, g, 9), rx03, -(((3.0 * x2) * rx0) * x3));
   const double cpf0 = rD, cpf1 = x3 * rD, cpf2 = x2 * rx0, cpf3 = rx0 * rx0;
 
-  // ---- explicit coupling + matrix of the implicit system, ascending j ----
+  // ---- explicit coupling + matrix of the implicit system over partners ----
   double g0 = 0.0, g1 = 0.0, tn = 0.0, tg2 = 0.0, tg3 = 0.0;
   double Am[KB], Bm[KB], Cm[KB], Dm[KB];
 #pragma unroll
-  for (int j = 0; j < KB; ++j) {
-    Am[j] = 0.0; Bm[j] = 0.0; Cm[j] = 0.0; Dm[j] = 0.0;
-    if (j < K) {
-      const int src = g.base + j;
-      // neighbour state; its coupling terms are recomputed exactly as the
+  for (int d = 1; d < KB; ++d) {
+    Am[d] = 0.0; Bm[d] = 0.0; Cm[d] = 0.0; Dm[d] = 0.0;
+    if (d < K) {
+      const int src = partner_lane(g, d);
+      // partner state; its coupling terms are recomputed exactly as the
       // owning lane computes them (cheaper than shuffling seven terms)
       const double xj0 = shfl(x0, src), xj1 = shfl(x1, src), xj2 = shfl(x2, src), xj3 = shfl(x3, src);
-      if (j != li && on) {
+      if (on) {
+        const int j = src - g.base;
         const double j02 = xj0 * xj0;
         const double j03 = j02 * xj0;
         const double h0j = xj0 * (xj2 * xj2);
@@ -307,10 +378,10 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const double*
         tn = fma(m1, t2, tn);
         tg2 = fma(m1, t1, tg2);
         tg3 = fma(m2, t1, tg3);
-        Am[j] = (m0 * rd) * j02;
-        Bm[j] = ((0.5 * m0) * srd2) * j03;
-        Cm[j] = -((m1 * srd2) * j02);
-        Dm[j] = -((m1 * rd3) * j03);
+        Am[d] = (m0 * rd) * j02;
+        Bm[d] = ((0.5 * m0) * srd2) * j03;
+        Cm[d] = -((m1 * srd2) * j02);
+        Dm[d] = -((m1 * rd3) * j03);
       }
     }
   }
@@ -328,13 +399,12 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const double*
     if (__all_sync(FULL, conv)) break;
     double ar = 0.0, at = 0.0;
 #pragma unroll
-    for (int j = 0; j < KB; ++j)
-      if (j < K) {
-        const double vrj = shfl(vr, g.base + j), vtj = shfl(vt, g.base + j);
-        if (j != li) {
-          ar = fma(Am[j], vrj, fma(Bm[j], vtj, ar));
-          at = fma(Cm[j], vrj, fma(Dm[j], vtj, at));
-        }
+    for (int d = 1; d < KB; ++d)
+      if (d < K) {
+        const int src = partner_lane(g, d);
+        const double vrj = shfl(vr, src), vtj = shfl(vt, src);
+        ar = fma(Am[d], vrj, fma(Bm[d], vtj, ar));
+        at = fma(Cm[d], vrj, fma(Dm[d], vtj, at));
       }
     const double ax0 = fma(ar, cpf0, vr);
     const double ax1 = at + vt;
@@ -389,18 +459,11 @@ __device__ __forceinline__ void prologue(LaneState& S, const Params& P, double g
   S.lin_iters = 0;
 }
 
-__device__ __forceinline__ void tally(LaneState& S, bool on, bool cv, int it, int& conv_fail_here) {
-  if (!on) return;
-  S.lin_iters += it;
-  if (cv) ++S.conv_ok;
-  else { ++S.conv_fail; ++conv_fail_here; }
-}
-
 // One adaptive Cash-Karp step for every active group of the warp
 // (stepper.py:362-677).  Returns true (per lane) if a dense sample must be
 // stored after this step; the caller writes it.
 template <int KB>
-__device__ __forceinline__ bool step(const Geo& g, const Params& P, const double* hc, const MView& M,
+__device__ __forceinline__ bool step(const Geo& g, const Params& P, const WarpSmem& W, const MView& M,
                                      LaneState& S) {
   const bool on = S.active;
   double h = S.h;
@@ -419,65 +482,67 @@ __device__ __forceinline__ bool step(const Geo& g, const Params& P, const double
     }
   }
   const double t = S.t;
-  const double* y = S.y;
-  double k1[4], k2[4], k3[4], k4[4], k5[4], k6[4], ys[4];
-  bool cv;
-  int it;
+  double* ks = W.ks + g.lane;   // ks[(st * 4 + c) * 32]
   int conv_fail_here = 0;
 
-  rhs<KB>(g, P, hc, M, S, on, t, y, k1, cv, it);
-  tally(S, on, cv, it, conv_fail_here);
+  // six Cash-Karp stages (stepper.py:379-480), one RHS call site
+#pragma unroll 1
+  for (int st = 0; st < 6; ++st) {
+    double ys[4];
+    if (st == 0) {
 #pragma unroll
-  for (int c = 0; c < 4; ++c) ys[c] = fma(h, B21 * k1[c], y[c]);
-  rhs<KB>(g, P, hc, M, S, on, fma(A2, h, t), ys, k2, cv, it);
-  tally(S, on, cv, it, conv_fail_here);
+      for (int c = 0; c < 4; ++c) ys[c] = S.y[c];
+    } else {
 #pragma unroll
-  for (int c = 0; c < 4; ++c) ys[c] = fma(h, fma(B32, k2[c], B31 * k1[c]), y[c]);
-  rhs<KB>(g, P, hc, M, S, on, fma(A3, h, t), ys, k3, cv, it);
-  tally(S, on, cv, it, conv_fail_here);
+      for (int c = 0; c < 4; ++c) {
+        double acc = kStageB[st][0] * ks[c * 32];
+        for (int m = 1; m < st; ++m) acc = fma(kStageB[st][m], ks[(m * 4 + c) * 32], acc);
+        ys[c] = fma(h, acc, S.y[c]);
+      }
+    }
+    const double ts = (st == 0) ? t : fma(kStageA[st], h, t);
+    double kk[4];
+    bool cv;
+    int it;
+    rhs<KB>(g, P, W, M, S.sp0, S.sp3, on, ts, ys, kk, cv, it);
 #pragma unroll
-  for (int c = 0; c < 4; ++c) ys[c] = fma(h, fma(B43, k3[c], fma(B42, k2[c], B41 * k1[c])), y[c]);
-  rhs<KB>(g, P, hc, M, S, on, fma(A4, h, t), ys, k4, cv, it);
-  tally(S, on, cv, it, conv_fail_here);
-#pragma unroll
-  for (int c = 0; c < 4; ++c)
-    ys[c] = fma(h, fma(B54, k4[c], fma(B53, k3[c], fma(B52, k2[c], B51 * k1[c]))), y[c]);
-  rhs<KB>(g, P, hc, M, S, on, fma(A5, h, t), ys, k5, cv, it);
-  tally(S, on, cv, it, conv_fail_here);
-#pragma unroll
-  for (int c = 0; c < 4; ++c)
-    ys[c] = fma(h, fma(B65, k5[c], fma(B64, k4[c], fma(B63, k3[c], fma(B62, k2[c], B61 * k1[c])))), y[c]);
-  rhs<KB>(g, P, hc, M, S, on, fma(A6, h, t), ys, k6, cv, it);
-  tally(S, on, cv, it, conv_fail_here);
+    for (int c = 0; c < 4; ++c) ks[(st * 4 + c) * 32] = kk[c];
+    if (on) {
+      S.lin_iters += it;
+      if (cv) ++S.conv_ok;
+      else {
+        ++S.conv_fail;
+        ++conv_fail_here;
+      }
+    }
+  }
 
-  // candidate (c2 = c5 = 0)
+  // candidate (c2 = c5 = 0) and embedded error estimate (ce2 = 0)
   double yn[4];
   bool fin = true;
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const double acc = fma(C6, k6[c], fma(C4, k4[c], fma(C3, k3[c], C1 * k1[c])));
-    yn[c] = fma(h, acc, y[c]);
-    fin = fin && cbcm::isfinite_(yn[c]);
-  }
-  const bool finite = group_all(fin, g);
-  if (on) ++S.steps;
-
-  const double g_new = group_event<KB>(yn, S.up[12], g, P.col);
-  const bool crossing = (S.g_old * g_new < 0.0);
-  // embedded error estimate, per lane (ce2 = 0)
   double ratio_l = 1.0e30;
   bool ok_l = true;
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    const double es = fma(CE6, k6[c], fma(CE5, k5[c], fma(CE4, k4[c], fma(CE3, k3[c], CE1 * k1[c]))));
+    const double k1 = ks[(0 * 4 + c) * 32], k3 = ks[(2 * 4 + c) * 32], k4 = ks[(3 * 4 + c) * 32],
+                 k5 = ks[(4 * 4 + c) * 32], k6 = ks[(5 * 4 + c) * 32];
+    const double acc = fma(C6, k6, fma(C4, k4, fma(C3, k3, C1 * k1)));
+    yn[c] = fma(h, acc, S.y[c]);
+    fin = fin && cbcm::isfinite_(yn[c]);
+    const double es = fma(CE6, k6, fma(CE5, k5, fma(CE4, k4, fma(CE3, k3, CE1 * k1))));
     const double e = fabs(h * es) + 1.0e-18;
-    const double ay = fabs(yn[c]), ao = fabs(y[c]);
+    const double ay = fabs(yn[c]), ao = fabs(S.y[c]);
     const double tl = P.rtol * (ay > ao ? ay : ao);
     const double tol = tl > P.atol ? tl : P.atol;
     const double r = tol / e;
     if (r < ratio_l) ratio_l = r;
     if (r < 1.0) ok_l = false;
   }
+  const bool finite = group_all(fin, g);
+  if (on) ++S.steps;
+
+  const double g_new = group_event<KB>(yn, upv(W, g, 12), g, P.col);
+  const bool crossing = (S.g_old * g_new < 0.0);
   const double ratio = group_min<KB>(ratio_l, g);
   const bool okerr = group_all(ok_l, g);
 
@@ -531,12 +596,12 @@ __device__ __forceinline__ bool step(const Geo& g, const Params& P, const double
     } else {
       store = ok && landing;
     }
-    // termination (stepper.py:651-662): evaluated after the caller stores
   }
   return store;
 }
 
-// After a dense store (if any): advance the schedule and test termination.
+// After a dense store (if any): advance the schedule and test termination
+// (stepper.py:651-662).
 __device__ __forceinline__ void after_store(LaneState& S, const Params& P, bool stored) {
   if (!S.active) return;
   if (stored) {

@@ -18,6 +18,7 @@
 #include "cbc_internal.h"
 #include "ensemble.h"
 
+
 namespace cbc {
 
 template <int KB>
@@ -33,7 +34,7 @@ __device__ __forceinline__ void ens_store_dense(const EnsLayout& E, const LaneSt
 // prologue.  Called only by lanes whose group claimed s.
 template <int KB>
 __device__ __forceinline__ void ens_load(const EnsLayout& E, const Params& P, const Geo& g, int s, LaneState& S,
-                                         MView& M, double* hc, long long& boff) {
+                                         MView& M, const WarpSmem& W, long long& boff) {
   boff = E.bubble_offset[s];
   const long long b = boff + g.li;
   const double2* st = reinterpret_cast<const double2*>(E.state + b * 4);
@@ -42,11 +43,7 @@ __device__ __forceinline__ void ens_load(const EnsLayout& E, const Params& P, co
   S.y[1] = s01.y;
   S.y[2] = s23.x;
   S.y[3] = s23.y;
-  const double* up = E.unit_params + b * E.up_stride;
-#pragma unroll
-  for (int p = 0; p < 13; ++p) S.up[p] = up[p];
-  S.c73 = S.up[7] * (1.0 / 3.0);
-  S.c47 = S.up[4] * S.up[7];
+  store_bubble_consts(W, g, E.unit_params + b * E.up_stride, 1);
   const double* sp = E.system_params + (long long)s * E.sp_stride;
   S.sp0 = sp[0];
   S.sp3 = sp[3];
@@ -60,7 +57,7 @@ __device__ __forceinline__ void ens_load(const EnsLayout& E, const Params& P, co
   M.m = E.coupling + E.coupling_offset[s] + g.li;
   M.sc = (long long)g.K * g.K;
   M.sj = g.K;
-  if (g.li == 0) store_harmonics(hc, g, sp[1], sp[2], sp[4], E.control_params + (long long)s * E.cp_stride, P.nk, 1);
+  if (g.li == 0) store_harmonics(W, g, sp[1], sp[2], sp[4], E.control_params + (long long)s * E.cp_stride, P.nk, 1);
 }
 
 template <int KB>
@@ -86,12 +83,12 @@ __device__ __forceinline__ void ens_writeback(const EnsLayout& E, const Params& 
 // Persistent worker: warps claim systems of bucket [begin, end) of the work
 // list until it is empty.  All systems of a bucket have the same K (<= KB).
 template <int KB>
-__global__ void __launch_bounds__(128) ensemble_kernel(EnsLayout E, Params P, const int* __restrict__ order,
+__global__ void __launch_bounds__(128, min_blocks_for(KB)) ensemble_kernel(EnsLayout E, Params P, const int* __restrict__ order,
                                                        int begin, int end, int K, int* head,
                                                        long long max_steps) {
   extern __shared__ double smem[];
   const Geo g = make_geo(K);
-  double* hc = smem + (threadIdx.x >> 5) * (HC_PER_K * P.nk * (32 / K));
+  const WarpSmem W = warp_smem(smem, K, P.nk);
   const int lane = threadIdx.x & 31;
   const bool leader = g.valid && g.li == 0;
 
@@ -126,11 +123,14 @@ __global__ void __launch_bounds__(128) ensemble_kernel(EnsLayout E, Params P, co
       }
       if (__any_sync(FULL, want && claim < 0)) drained = true;
       // hand the claimed system id to every lane of the group
+      // (both shuffles are executed by every lane: never inside a
+      // short-circuit or a divergent branch)
       const int got = __shfl_sync(FULL, claim, g.base);
-      const bool fresh = g.valid && sys < 0 && got >= 0 && __shfl_sync(FULL, (int)want, g.base);
+      const int leader_wanted = __shfl_sync(FULL, (int)want, g.base);
+      const bool fresh = g.valid && sys < 0 && got >= 0 && leader_wanted != 0;
       if (fresh) {
         sys = got;
-        ens_load<KB>(E, P, g, sys, S, M, hc, boff);
+        ens_load<KB>(E, P, g, sys, S, M, W, boff);
       }
       __syncwarp();
       // first dense sample and initial event value for the fresh systems
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(128) ensemble_kernel(EnsLayout E, Params P, co
           }
         }
       }
-      const double g0 = group_event<KB>(S.y, S.up[12], g, P.col);
+      const double g0 = group_event<KB>(S.y, upv(W, g, 12), g, P.col);
       if (fresh && S.active) S.g_old = g0;
       // systems that arrive already finished go straight back out
       continue;
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(128) ensemble_kernel(EnsLayout E, Params P, co
       continue;
     }
     // ---- one Cash-Karp step for every active slot ----
-    const bool stq = step<KB>(g, P, hc, M, S);
+    const bool stq = step<KB>(g, P, W, M, S);
     if (stq) ens_store_dense<KB>(E, S, g, sys, boff, S.idx);
     after_store(S, P, stq);
     if (S.active && S.steps >= max_steps) {
@@ -170,7 +170,11 @@ __global__ void __launch_bounds__(128) ensemble_kernel(EnsLayout E, Params P, co
 template <int KB>
 cudaError_t launch_ensemble(const EnsLayout& E, const Params& P, const int* order, int begin, int end, int K,
                             int* head, long long max_steps, int blocks, int threads, cudaStream_t stream) {
-  const size_t shmem = sizeof(double) * (size_t)(HC_PER_K * P.nk * (32 / K)) * (threads / 32);
+  const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, P.nk) * (threads / 32);
+  if (shmem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(ensemble_kernel<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+    if (e != cudaSuccess) return e;
+  }
   ensemble_kernel<KB><<<blocks, threads, shmem, stream>>>(E, P, order, begin, end, K, head, max_steps);
   return cudaGetLastError();
 }
@@ -188,9 +192,18 @@ cudaError_t launch_ensemble_bucket(const EnsLayout& E, const Params& P, const in
 }
 
 int resident_blocks(int K, int nk, int threads) {
-  const size_t shmem = sizeof(double) * (size_t)(HC_PER_K * nk * (32 / K)) * (threads / 32);
+  const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, nk) * (threads / 32);
   int n = 0;
   cudaError_t e;
+  if (shmem > 48 * 1024) {
+    switch (kb_for(K)) {
+      case 2: cudaFuncSetAttribute(ensemble_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem); break;
+      case 4: cudaFuncSetAttribute(ensemble_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem); break;
+      case 8: cudaFuncSetAttribute(ensemble_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem); break;
+      case 16: cudaFuncSetAttribute(ensemble_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem); break;
+      default: cudaFuncSetAttribute(ensemble_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem); break;
+    }
+  }
   switch (kb_for(K)) {
     case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<2>, threads, shmem); break;
     case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<4>, threads, shmem); break;

@@ -34,9 +34,6 @@ struct RefLayout {
   long long* lin_iters;
 };
 
-// Shared memory per warp for the harmonic constants of its groups.
-__host__ __device__ inline int hc_doubles_per_warp(int K, int nk) { return HC_PER_K * nk * (32 / K); }
-
 template <int KB>
 __device__ __forceinline__ void ref_store_dense(const RefLayout& L, const LaneState& S, const Geo& g,
                                                 long long s, int slot) {
@@ -47,11 +44,11 @@ __device__ __forceinline__ void ref_store_dense(const RefLayout& L, const LaneSt
 }
 
 template <int KB>
-__global__ void __launch_bounds__(128) plain_kernel(RefLayout L, Params P, long long budget, int final_launch,
+__global__ void __launch_bounds__(128, min_blocks_for(KB)) plain_kernel(RefLayout L, Params P, long long budget, int final_launch,
                                                     int* active_counter) {
   extern __shared__ double smem[];
   const Geo g = make_geo(L.ups);
-  double* hc = smem + (threadIdx.x >> 5) * hc_doubles_per_warp(L.ups, P.nk);
+  const WarpSmem W = warp_smem(smem, L.ups, P.nk);
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long s = warp * g.G + g.grp;
   const bool have = g.valid && s < L.ns;
@@ -69,10 +66,7 @@ __global__ void __launch_bounds__(128) plain_kernel(RefLayout L, Params P, long 
   if (have) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) S.y[c] = L.actual_state[c * NST + lane_off];
-#pragma unroll
-    for (int p = 0; p < 13; ++p) S.up[p] = L.unit_params[p * NST + lane_off];
-    S.c73 = S.up[7] * (1.0 / 3.0);
-    S.c47 = S.up[4] * S.up[7];
+    store_bubble_consts(W, g, L.unit_params + lane_off, NST);
     S.sp0 = L.system_params[0 * (long long)L.ns + s];
     S.sp3 = L.system_params[3 * (long long)L.ns + s];
     S.t = L.actual_time[s];
@@ -84,7 +78,7 @@ __global__ void __launch_bounds__(128) plain_kernel(RefLayout L, Params P, long 
     const double prev = (P.ndo > 0 && S.idx > 0) ? L.dense_time[(long long)(S.idx - 1) * L.ns + s] : 0.0;
     prologue(S, P, g_store, prev, L.status[s]);
     if (g.li == 0)
-      store_harmonics(hc, g, L.system_params[1 * (long long)L.ns + s], L.system_params[2 * (long long)L.ns + s],
+      store_harmonics(W, g, L.system_params[1 * (long long)L.ns + s], L.system_params[2 * (long long)L.ns + s],
                       L.system_params[4 * (long long)L.ns + s], L.control_params + s, P.nk, L.ns);
   }
   __syncwarp();
@@ -104,13 +98,13 @@ __global__ void __launch_bounds__(128) plain_kernel(RefLayout L, Params P, long 
     }
   }
   {
-    const double g0 = group_event<KB>(S.y, S.up[12], g, P.col);
+    const double g0 = group_event<KB>(S.y, upv(W, g, 12), g, P.col);
     if (S.active) S.g_old = g0;
   }
 
   for (long long it = 0; it < budget; ++it) {
     if (!__any_sync(FULL, S.active)) break;
-    const bool st = step<KB>(g, P, hc, M, S);
+    const bool st = step<KB>(g, P, W, M, S);
     if (st) ref_store_dense<KB>(L, S, g, s, S.idx);
     after_store(S, P, st);
   }
@@ -142,7 +136,11 @@ cudaError_t launch_plain(const RefLayout& L, const Params& P, long long budget, 
   const long long warps = (L.ns + G - 1) / G;
   const int threads = 128;
   const long long blocks = (warps * 32 + threads - 1) / threads;
-  const size_t shmem = sizeof(double) * (size_t)hc_doubles_per_warp(L.ups, P.nk) * (threads / 32);
+  const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(L.ups, P.nk) * (threads / 32);
+  if (shmem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(plain_kernel<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+    if (e != cudaSuccess) return e;
+  }
   plain_kernel<KB><<<(unsigned)blocks, threads, shmem, stream>>>(L, P, budget, final_launch, counter);
   return cudaGetLastError();
 }
@@ -181,9 +179,16 @@ int32_t cbc_create(cbc_context** out, int32_t device) {
   cudaSetDevice(device);
   cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
   e = cudaMalloc(&ctx->d_counter, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_head, sizeof(int) * CBC_MAX_BUCKETS);
   if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_counter, sizeof(int));
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming);
+  for (int i = 0; i < CBC_SIDE_STREAMS && e == cudaSuccess; ++i) {
+    e = cudaEventCreateWithFlags(&ctx->join[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking);
+  }
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->capture, cudaStreamNonBlocking);
   cudaSetDevice(prev);
   if (e != cudaSuccess) {
     cbc_destroy(ctx);
@@ -199,9 +204,16 @@ int32_t cbc_destroy(cbc_context* ctx) {
   cudaGetDevice(&prev);
   cudaSetDevice(ctx->device);
   if (ctx->d_counter) cudaFree(ctx->d_counter);
+  if (ctx->d_head) cudaFree(ctx->d_head);
   if (ctx->h_counter) cudaFreeHost(ctx->h_counter);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->fork) cudaEventDestroy(ctx->fork);
+  for (int i = 0; i < CBC_SIDE_STREAMS; ++i) {
+    if (ctx->join[i]) cudaEventDestroy(ctx->join[i]);
+    if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
+  }
+  if (ctx->capture) cudaStreamDestroy(ctx->capture);
   cudaSetDevice(prev);
   delete ctx;
   return CBC_OK;

@@ -139,6 +139,113 @@ int32_t cbc_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_buffers* buf
                   int64_t max_steps, int32_t kernel_steps, int32_t launch_mode, void* stream,
                   cbc_solve_stats* stats);
 
+/* ---- batched mixed-K form --------------------------------------------------
+ * A ragged ensemble: systems of different bubble counts K (1..32) in one set of
+ * arrays.  Bubbles of system s are bubble_offset[s] .. bubble_offset[s]+K_s-1.
+ * Layout (device memory, row-major, f64 unless noted):
+ *   bubble_offset, coupling_offset   (ns) i64
+ *   state                            (nb, 4)         R, X, U, V; 16-byte aligned
+ *   unit_params                      (nb, up_stride) the 13 constants of
+ *                                                    models/ckm1d.py:154-168
+ *   system_params                    (ns, sp_stride) the 5 constants of ckm1d.py:171-175
+ *   control_params                   (ns, cp_stride) PA[nk], omega[nk], phase[nk], wave[nk]
+ *   coupling                         per system at coupling_offset[s]: (3, K, K),
+ *                                    [c][j][i] = matrix c, source j, receiver i
+ *   t, t_end, t_begin, h, event      (ns)
+ *   status, dense_index              (ns) i32
+ *   dense_time                       (ndo, ns)       sample-major
+ *   dense_state                      (ndo, nb, 4)    sample-major; 16-byte aligned
+ *   steps, rejected, conv_ok, conv_fail (ns) i32, lin_iters (ns) i64: optional
+ * The spec's ns, ups and tile fields are ignored; its solver fields, nk, ac,
+ * ndo and dense_mode apply to every system. */
+typedef struct cbc_ensemble {
+  int32_t ns;
+  int32_t up_stride, sp_stride, cp_stride;
+  int64_t nb;
+  const int64_t* bubble_offset;
+  const int64_t* coupling_offset;
+  double* state;
+  const double* unit_params;
+  const double* system_params;
+  const double* control_params;
+  const double* coupling;
+  double* t;
+  const double* t_end;
+  const double* t_begin;
+  double* h;
+  double* event;
+  int32_t* status;
+  int32_t* dense_index;
+  double* dense_time;
+  double* dense_state;
+  int32_t* steps;
+  int32_t* rejected;
+  int32_t* conv_ok;
+  int32_t* conv_fail;
+  int64_t* lin_iters;
+} cbc_ensemble;
+
+/* Work list: system ids grouped in buckets of equal K (device array `order`),
+ * each bucket ordered longest expected work first.  bucket_K, bucket_begin
+ * (nbuckets + 1 entries), and the optional tuning arrays threads (per-block
+ * threads, 32..128) and blocks_per_sm are host arrays. */
+typedef struct cbc_work {
+  const int32_t* order;
+  int32_t nbuckets;
+  const int32_t* bucket_K;
+  const int32_t* bucket_begin;
+  const int32_t* threads;
+  const int32_t* blocks_per_sm;
+} cbc_work;
+
+typedef struct cbc_plan cbc_plan;
+
+/* Advances every system of the ensemble by at most max_steps steps (per
+ * system, per call) or until it finishes.  One persistent work-stealing kernel
+ * per bucket, buckets on forked streams that join back into `stream`.
+ * Results are bit-identical to cbc_solve on the same systems.  No reference
+ * counterpart: the reference integrates one (NS, K) shape per kernel build
+ * (backends/cupy_cuda/kernel_loader.py:35-63); this is its batched form. */
+int32_t cbc_ensemble_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* ens,
+                           const cbc_work* work, int64_t max_steps, void* stream);
+
+/* Captures the same launch sequence into a CUDA graph bound to these buffers;
+ * cbc_plan_launch replays it on `stream` (one graph launch per solve). */
+int32_t cbc_plan_create(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* ens,
+                        const cbc_work* work, int64_t max_steps, cbc_plan** out);
+int32_t cbc_plan_launch(cbc_plan* plan, void* stream);
+int32_t cbc_plan_destroy(cbc_plan* plan);
+
+/* ---- vec-env step ------------------------------------------------------------
+ * Device buffers of one environment step around the batched solve (uniform K,
+ * one system per environment, ns * K == nb).  Before the solve, for every env
+ * s: control_params[s][a] = actions[s * act_stride + a] * act_scale for
+ * a < n_act (the PA columns: bar -> Pa with act_scale 1e5), t = 0,
+ * t_end = t_span, h = h0, event = -1, status = 0.  After the solve:
+ * obs[s][0..K-1] = x, obs[s][K..2K-1] = R (float32), failed[s] = status != 1
+ * (failed may be NULL).  Reference: PosNBC1D.step
+ * (envs/bubble_1D_pos_control.py:503-538: set_action :732-749,
+ * advance_time :816-826, check_termination :772-789, observe :756-769). */
+typedef struct cbc_env_io {
+  const float* actions;
+  int32_t n_act;
+  int32_t act_stride;
+  double act_scale;
+  float* obs;
+  uint8_t* failed;
+  int32_t K;
+  int32_t pad;
+  double t_span;
+  double h0;
+} cbc_env_io;
+
+/* A plan whose graph is env prologue -> batched solve -> env epilogue; one
+ * cbc_plan_launch is one environment step for every env (io == NULL gives
+ * the plain cbc_plan_create graph). */
+int32_t cbc_env_plan_create(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* ens,
+                            const cbc_work* work, int64_t max_steps, const cbc_env_io* io,
+                            cbc_plan** out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -127,6 +127,18 @@ struct Spec {
   int lin_max_iter, ndo, dense_mode;
 };
 
+// Pairwise-tree sum over the next power of two (zero padded):
+// ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + ...).
+double tree_sum(const double* a, int K) {
+  int P = 1;
+  while (P < K) P <<= 1;
+  double buf[2 * KMAX];
+  for (int i = 0; i < P; ++i) buf[i] = i < K ? a[i] : 0.0;
+  for (int w = 1; w < P; w <<= 1)
+    for (int i = 0; i < P; i += 2 * w) buf[i] = buf[i] + buf[i + w];
+  return buf[0];
+}
+
 // ode_fun + explicit_coupling + implicit_coupling for the whole system
 // (ckm1d_def.py:408-497, :164-248, :250-300, :303-404).
 void rhs(const System& s, const Spec& sp, double t, const double (*y)[4], double (*dy)[4],
@@ -203,7 +215,8 @@ void rhs(const System& s, const Spec& sp, double t, const double (*y)[4], double
   }
 
   // explicit coupling (ckm1d_def.py:164-246) and the matrix of the implicit
-  // system (mat_vec_product, ckm1d_def.py:250-299), ascending j, diagonal skipped
+  // system (mat_vec_product, ckm1d_def.py:250-299).  Canonical order: bubble i
+  // sums over its partners j = (i + d) mod K, d = 1 .. K-1.
   static thread_local std::vector<double> Am, Bm, Cm, Dm;
   Am.resize((size_t)K * K);
   Bm.resize((size_t)K * K);
@@ -212,8 +225,8 @@ void rhs(const System& s, const Spec& sp, double t, const double (*y)[4], double
   for (int i = 0; i < K; ++i) {
     const double xi = y[i][1];
     double g0 = 0.0, g1 = 0.0, tn = 0.0, tg2 = 0.0, tg3 = 0.0;
-    for (int j = 0; j < K; ++j) {
-      if (j == i) continue;
+    for (int d = 1; d < K; ++d) {
+      const int j = (i + d) % K;
       const double delta = xi - y[j][1];
       const double sg = (double)((delta > 0.0) - (delta < 0.0));
       const double ad = fabs(delta);
@@ -240,9 +253,11 @@ void rhs(const System& s, const Spec& sp, double t, const double (*y)[4], double
     b1[i] = b1[i] + fma(tg2, cpf2[i], fma(tg3, cpf3[i], tn));
   }
 
-  // implicit coupling: relaxed Richardson from v = b (ckm1d_def.py:303-404)
-  double bn = 0.0;
-  for (int i = 0; i < K; ++i) bn = bn + fma(b0[i], b0[i], b1[i] * b1[i]);
+  // implicit coupling: relaxed Richardson from v = b (ckm1d_def.py:303-404);
+  // norms are pairwise-tree sums over the bubbles
+  double acc[KMAX];
+  for (int i = 0; i < K; ++i) acc[i] = fma(b0[i], b0[i], b1[i] * b1[i]);
+  const double bn = tree_sum(acc, K);
   const double rt = sp.lin_rtol2 * bn;
   const double tol2 = rt > sp.lin_atol2 ? rt : sp.lin_atol2;
   double vr[KMAX], vt[KMAX], r0[KMAX], r1[KMAX];
@@ -252,11 +267,10 @@ void rhs(const System& s, const Spec& sp, double t, const double (*y)[4], double
   }
   bool conv = false;
   for (int it = 0; it < sp.lin_max_iter; ++it) {
-    double rn = 0.0;
     for (int i = 0; i < K; ++i) {
       double ar = 0.0, at = 0.0;
-      for (int j = 0; j < K; ++j) {
-        if (j == i) continue;
+      for (int d = 1; d < K; ++d) {
+        const int j = (i + d) % K;
         ar = fma(Am[(size_t)i * K + j], vr[j], fma(Bm[(size_t)i * K + j], vt[j], ar));
         at = fma(Cm[(size_t)i * K + j], vr[j], fma(Dm[(size_t)i * K + j], vt[j], at));
       }
@@ -265,7 +279,8 @@ void rhs(const System& s, const Spec& sp, double t, const double (*y)[4], double
       r0[i] = b0[i] - ax0;
       r1[i] = b1[i] - ax1;
     }
-    for (int i = 0; i < K; ++i) rn = rn + fma(r0[i], r0[i], r1[i] * r1[i]);
+    for (int i = 0; i < K; ++i) acc[i] = fma(r0[i], r0[i], r1[i] * r1[i]);
+    const double rn = tree_sum(acc, K);
     cnt.lin_iters += 1;
     if (rn < tol2) {
       conv = true;

@@ -98,6 +98,14 @@ CASES = [
 ]
 
 
+# Longer spans (a few hundred to a thousand steps, through a collapse for the
+# driven cases).  Written to golden_ref_numba_long.npz with GOLDEN_SET=long.
+CASES_LONG = [
+    ("k2_swa_long", 2, "SW_A", 2, [6.0, 4.0], [1.3, 0.8], [25.0, 50.0], [0.7, 1.6], [-0.1, 0.02], 0.06),
+    ("k2_const_long", 2, "CONST", 1, [7.0, 5.0], [-1.2156], [20.0], [0.0], [0.0, 200e-6 / (1497.0 / 20e3)], 0.06),
+]
+
+
 def run_case(case, water):
     from coupledbubble_control.models import CKM1D, MaterialProperties
     from coupledbubble_control.backends import BackendName, KernelVariant
@@ -133,7 +141,8 @@ def main():
     install_shims()
     sys.path.insert(0, REF)
     out = {}
-    for case in CASES:
+    long_set = os.environ.get("GOLDEN_SET", "") == "long"
+    for case in (CASES_LONG if long_set else CASES):
         print("running", case[0], flush=True)
         init, final, meta = run_case(case, water=True)
         for k, v in init.items():
@@ -142,8 +151,9 @@ def main():
             out[f"{meta['name']}/final/{k}"] = v
         out[f"{meta['name']}/meta"] = np.array([meta["K"], meta["nk"], ["CONST", "SW_N", "SW_A"].index(meta["ac"])])
         print("  t", final["actual_time"], "R", final["actual_state"][0, 0, :meta["K"]], flush=True)
-    np.savez_compressed(os.path.join(HERE, "golden_ref_numba.npz"), **out)
-    print("wrote", os.path.join(HERE, "golden_ref_numba.npz"))
+    fn = os.path.join(HERE, "golden_ref_numba_long.npz" if long_set else "golden_ref_numba.npz")
+    np.savez_compressed(fn, **out)
+    print("wrote", fn)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,61 @@
+"""Pins the CPU oracle to the reference implementation.
+
+tests/golden/golden_ref_numba.npz holds the initial buffers and the final
+buffers of the reference's own CKM1D model integrated by its numba backend
+(rkck45_coupled_numba_stepper.py), executed by numba's CUDA simulator
+(generator: tests/golden/make_golden.py).  The oracle starts from the same
+buffers and must land on the same end time and state.
+
+Tolerance: the reference evaluates with numpy's libm and without fused
+multiply-adds, the oracle with cbc_math and explicit fma, so they differ at
+the rounding level (~1e-16 per operation).  Over the few hundred steps of a
+case this stays far below the integrator tolerance: we require relative
+agreement 1e-11 on every state component (floor 1e-12 absolute; observed
+<= 5e-14) and identical
+end times and statuses.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from cbc_b200.models import SolverSpec
+from oracle import oracle
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden", "golden_ref_numba.npz")
+AC = ["CONST", "SW_N", "SW_A"]
+
+
+def load_cases():
+    import glob
+    out = []
+    for fn in sorted(glob.glob(os.path.join(HERE, "golden", "golden_ref_numba*.npz"))):
+        z = np.load(fn)
+        out += [(n, z) for n in sorted({k.split("/")[0] for k in z.files})]
+    return out
+
+
+@pytest.mark.parametrize("name,z", load_cases(), ids=lambda v: v if isinstance(v, str) else "")
+def test_oracle_matches_reference_numba(name, z):
+    K, nk, ac = (int(v) for v in z[f"{name}/meta"])
+    init = {k.split("/", 2)[2]: np.array(z[k]) for k in z.files if k.startswith(f"{name}/init/")}
+    final = {k.split("/", 2)[2]: np.array(z[k]) for k in z.files if k.startswith(f"{name}/final/")}
+    ns, tile = init["actual_state"].shape[1], init["actual_state"].shape[2]
+    buf = {k: np.ascontiguousarray(v) for k, v in init.items()}
+    buf["lin_iters"] = np.zeros(ns, np.int64)
+    spec = oracle.make_spec(ns, K, tile, 0, nk, AC[ac], SolverSpec())
+    oracle.solve_ref_layout(spec, buf, 1_000_000)
+    assert np.all(buf["status_flags"] == final["status_flags"]), (buf["status_flags"], final["status_flags"])
+    np.testing.assert_allclose(buf["actual_time"], final["actual_time"], rtol=0, atol=1e-15)
+    a = buf["actual_state"][:, :, :K]
+    b = final["actual_state"][:, :, :K]
+    err = np.abs(a - b) / np.maximum(np.abs(b), 1e-12)
+    assert np.max(err) < 1e-11, f"max relative state error {np.max(err):.3e}"
+    # event value (collision gap) agrees to the same level
+    if K > 1:
+        np.testing.assert_allclose(buf["actual_event"], final["actual_event"], rtol=1e-9)
+
+
+def test_golden_file_present():
+    assert os.path.exists(GOLDEN), "run tests/golden/make_golden.py in a container that has the reference"
