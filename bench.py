@@ -145,29 +145,34 @@ def measured_fp64_peak(dev) -> float:
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_baseline(scene, seconds_hint: float = 15.0, nthreads: int = 0):
+def cpu_baseline(scene, seconds: float = 12.0, nthreads: int = 0, seed: int = 99):
     """The CPU oracle (C++ restatement of the reference integrator, all host
-    cores) on a bounded stratified sample of the same workload."""
+    cores) on a bounded random sample of the same workload: batches of 64
+    systems (spans capped at 5 periods) until `seconds` of CPU time are spent."""
     from cbc_b200 import scenes
     from oracle import oracle
-    rng = np.random.default_rng(99)
-    n = 96
-    idx = np.sort(rng.choice(scene.ns, size=n, replace=False))
-    sub = scenes.subset(scene, idx)
-    cap = 2.0
-    sub.t_end = np.minimum(sub.t_end, cap)
-    total_adv = 0.0
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(scene.ns)
+    cap = 5.0
+    total_adv, n_done, pos = 0.0, 0, 0
     t0 = time.perf_counter()
-    for k in np.unique(sub.K):
-        sel = np.nonzero(sub.K == k)[0]
-        m = scenes.build_model(scenes.subset(sub, sel), ndo=0)
-        buf = oracle.solve_model(m, max_steps=MAX_STEPS, kernel_steps=MAX_STEPS, nthreads=nthreads)
-        total_adv += float(np.sum(buf["actual_time"]))
+    while time.perf_counter() - t0 < seconds and pos < scene.ns:
+        idx = np.sort(perm[pos:pos + 64])
+        pos += 64
+        sub = scenes.subset(scene, idx)
+        sub.t_end = np.minimum(sub.t_end, cap)
+        for k in np.unique(sub.K):
+            sel = np.nonzero(sub.K == k)[0]
+            m = scenes.build_model(scenes.subset(sub, sel), ndo=0)
+            buf = oracle.solve_model(m, max_steps=MAX_STEPS, kernel_steps=MAX_STEPS, nthreads=nthreads)
+            total_adv += float(np.sum(buf["actual_time"]))
+        n_done += idx.size
     dt = time.perf_counter() - t0
     cores = nthreads if nthreads > 0 else (os.cpu_count() or 1)
     return {"value": total_adv / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} systems drawn from the same mixed-K ensemble, spans capped at {cap} periods "
-                      f"({total_adv:.1f} system-periods in {dt:.1f} s), CPU oracle on {cores} threads"}
+            "sample": f"{n_done} systems drawn at random from the same mixed-K ensemble, spans capped at "
+                      f"{cap} periods ({total_adv:.1f} system-periods in {dt:.1f} s), CPU oracle "
+                      f"(C++ restatement of the reference integrator) on {cores} threads"}
 
 
 def run_reference(args):
@@ -191,6 +196,22 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def batched_once(scene, dev_index: int, schedule: str) -> float:
+    """System-periods/s of one batched solve of `scene` (for the ratio)."""
+    import torch
+    from cbc_b200.ensemble import Ensemble
+    ens = Ensemble.from_scene(scene, device=dev_index).to_device()
+    plan = ens.scheduled_plan(MAX_STEPS, 256) if schedule == "pilot" else ens.plan(MAX_STEPS)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plan.launch()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    adv = float((ens.dev["t"] - torch.from_numpy(ens.host["t"]).to(ens.dev["t"].device)).sum().item())
+    plan.close()
+    return adv / dt
+
+
 def plain_per_k(scene, dev):
     """The reference execution model on the same systems: one reference-layout
     solve per K (cbc_solve, relaunch every 2048 steps with a host check)."""
@@ -211,6 +232,35 @@ def plain_per_k(scene, dev):
     return adv / total, total
 
 
+def env_step_latency(dev_index: int, n_steps: int = 128, warmup: int = 3):
+    """PPO vec-env stepping: 1024 envs x K=4 bubbles (R0 60 um, SW_N, 25+50 kHz),
+    5 periods per env step, actions (PA_1, PA_2) ~ U[0, 1.5] bar from seed 2,
+    float32 observation written in place, 128-step horizon with resets.
+    Returns p50/p95/p99 of the env-step time measured with CUDA events."""
+    import torch
+    from cbc_b200.envs import CKM1DVecEnv
+    env = CKM1DVecEnv(num_envs=1024, num_bubbles=4, time_step_length=5.0, episode_length=128, seed=42,
+                      device=dev_index)
+    env.reset()
+    gen = torch.Generator(device=torch.device("cuda", dev_index)).manual_seed(2)
+    times = []
+    for i in range(warmup + n_steps):
+        act = torch.rand((1024, 2), device=torch.device("cuda", dev_index), generator=gen) * 1.5
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        env.step(act)
+        b.record()
+        b.synchronize()
+        if i >= warmup:
+            times.append(a.elapsed_time(b))
+    env.close()
+    t = np.asarray(times)
+    return {"p50_ms": float(np.percentile(t, 50)), "p95_ms": float(np.percentile(t, 95)),
+            "p99_ms": float(np.percentile(t, 99)), "mean_ms": float(t.mean()), "steps": int(t.size),
+            "envs": 1024, "K": 4, "periods_per_step": 5.0,
+            "env_system_periods_per_s": float(1024 * 5.0 / (t.mean() * 1e-3))}
+
+
 def run_b200(args):
     import torch
     rank, world, local = dist_env()
@@ -228,7 +278,7 @@ def run_b200(args):
     scene = scenes.mixed_k(ns=args.ns, seed=rank_seed(rank))
     ens = Ensemble.from_scene(scene, device=local)
     ens.to_device()
-    plan = ens.plan(MAX_STEPS)
+    plan = ens.scheduled_plan(MAX_STEPS, pilot_steps=256) if args.schedule == "pilot" else ens.plan(MAX_STEPS)
     nbuckets = int(np.unique(scene.K).size)
     # pristine device copy of the initial state for the per-step reset
     pristine = {k: v.clone() for k, v in ens.dev.items()}
@@ -282,7 +332,7 @@ def run_b200(args):
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        for _ in range(args.steps):
+        for _ in range(args.e2e_steps):
             for k in keys_in:
                 ens.dev[k].copy_(pin_in[k], non_blocking=True)
             flush.fill_(1.0)
@@ -292,14 +342,23 @@ def run_b200(args):
         b.record()
         torch.cuda.synchronize()
         e2e_ms = a.elapsed_time(b)
-        e2e = {"value": adv * args.steps / (e2e_ms * 1e-3) * (world if pg else 1), "unit": UNIT,
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+        e2e = {"value": adv * args.e2e_steps / (e2e_ms * 1e-3) * (world if pg else 1), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps}
+
+    env_lat = None
+    if args.env and rank == 0:
+        env_lat = env_step_latency(local)
 
     plain = None
     if args.plain and rank == 0:
-        pv, ptime = plain_per_k(scene, dev)
-        plain = {"value": pv, "unit": UNIT, "seconds": ptime,
-                 "how": "reference-layout solve per K (relaunch every 2048 steps + host completion check)"}
+        from cbc_b200 import scenes as _sc
+        sub = _sc.subset(scene, np.arange(min(args.plain_ns, scene.ns)))
+        pv, ptime = plain_per_k(sub, dev)
+        bv = batched_once(sub, local, args.schedule)
+        plain = {"value": pv, "unit": UNIT, "seconds": ptime, "systems": sub.ns, "batched_same_systems": bv,
+                 "how": "reference-layout solve per K (relaunch every 2048 steps + host completion check) "
+                        "on the first systems of the same ensemble; batched_same_systems is the batched "
+                        "form on exactly those systems"}
 
     if rank == 0:
         peak = measured_fp64_peak(dev)
@@ -312,7 +371,8 @@ def run_b200(args):
             "config": {"workload": f"mixed_k_{args.ns}", "ns_per_gpu": args.ns, "K": [2, 3, 4, 6, 8],
                        "K_weights": [0.4, 0.2, 0.2, 0.1, 0.1], "span_periods": [5, 50], "rtol": 1e-9,
                        "atol": 1e-9, "max_steps": MAX_STEPS, "field": "SW_A 25+50 kHz",
-                       "l2": "256 MiB buffer written before every step", "parallelism": f"replicas{world}"},
+                       "l2": "256 MiB buffer written before every step", "parallelism": f"replicas{world}",
+                       "schedule": args.schedule},
             "work": {"advanced_system_periods_per_step": adv, "nominal_system_periods": float(np.sum(scene.t_end)),
                      "status_counts": status, "steps_per_solve": int(np.sum(res["steps"])),
                      "richardson_sweeps_per_rhs": float(np.sum(res["lin_iters"]) / max(1, 6 * np.sum(res["steps"]))),
@@ -322,13 +382,15 @@ def run_b200(args):
                          "note": "algorithmic FP64 flops (transcendentals counted as 1) / graph time; "
                                  "peak = cuBLAS FP64 GEMM measured in this run"},
             "clocks": clk.summary(),
-            "gpu_launches": args.steps * nbuckets,
+            "gpu_launches": args.steps * nbuckets * (2 if args.schedule == "pilot" else 1),
         }
         if plain:
             line["plain"] = plain
-            line["batched_vs_plain"] = value / world / plain["value"]
+            line["batched_vs_plain"] = plain["batched_same_systems"] / plain["value"]
         if e2e:
             line["e2e"] = e2e
+        if env_lat:
+            line["env_step_latency"] = env_lat
         if world == 1 and args.cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(scene)
         print(json.dumps(line), flush=True)
@@ -348,6 +410,11 @@ def main():
     ap.add_argument("--no-plain", dest="plain", action="store_false")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-env", dest="env", action="store_false")
+    ap.add_argument("--plain-ns", type=int, default=16384, help="systems used for the batched-vs-plain ratio")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--schedule", default="pilot", choices=["pilot", "span"],
+                    help="pilot: measured longest-first re-ordering after a pilot pass; span: longest span first")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

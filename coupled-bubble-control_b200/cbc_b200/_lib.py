@@ -51,12 +51,12 @@ class cbc_ensemble(ctypes.Structure):
         [(n, P) for n in ("bubble_offset", "coupling_offset", "state", "unit_params", "system_params",
                           "control_params", "coupling", "t", "t_end", "t_begin", "h", "event", "status",
                           "dense_index", "dense_time", "dense_state", "steps", "rejected", "conv_ok",
-                          "conv_fail", "lin_iters")]
+                          "conv_fail", "lin_iters", "trace_load_ns", "trace_done_ns")]
 
 
 class cbc_work(ctypes.Structure):
     _fields_ = [("order", P), ("nbuckets", i32), ("bucket_K", P), ("bucket_begin", P), ("threads", P),
-                ("blocks_per_sm", P)]
+                ("blocks_per_sm", P), ("share", P)]
 
 
 class cbc_env_io(ctypes.Structure):

@@ -33,32 +33,53 @@ class WorkList:
     bucket_begin: np.ndarray   # (nb + 1,) int32
     threads: Optional[np.ndarray] = None
     blocks_per_sm: Optional[np.ndarray] = None
+    share: Optional[np.ndarray] = None   # (nb,) float32 fraction of the GPU per bucket at the start
 
 
-def cost_weight(K: np.ndarray) -> np.ndarray:
-    """Relative work of one step of a K-bubble system: RHS per bubble plus
-    K^2 coupling pairs, each over ~14 Richardson sweeps."""
-    K = np.asarray(K, dtype=np.float64)
-    return 130.0 * K + 35.0 * K ** 2 + 14.0 * (20.0 * K ** 2 + 12.0 * K)
+# Steady-state cost of one system-step on a full B200 (ns), measured on
+# ensembles of identical systems (no tail); other K are interpolated.
+STEP_NS = {1: 0.6, 2: 0.995, 3: 2.65, 4: 3.13, 6: 9.24, 8: 12.6}
 
 
-def make_work_list(K: np.ndarray, span: np.ndarray, active: Optional[np.ndarray] = None) -> WorkList:
+def cost_weight(K) -> np.ndarray:
+    """Relative cost of one step of a K-bubble system (ns on a full GPU)."""
+    K = np.atleast_1d(np.asarray(K, dtype=np.float64))
+    ks = np.asarray(sorted(STEP_NS), dtype=np.float64)
+    vs = np.asarray([STEP_NS[int(k)] for k in ks])
+    out = np.interp(K, ks, vs)
+    big = K > ks[-1]
+    out[big] = vs[-1] * (K[big] / ks[-1]) ** 2
+    return out
+
+
+def make_work_list(K: np.ndarray, work: np.ndarray, active: Optional[np.ndarray] = None,
+                   shares: bool = True) -> WorkList:
     """Buckets of equal K, most expensive bucket first; inside a bucket the
-    systems with the longest remaining span come first (longest-processing-
-    time-first keeps the final tail short)."""
+    systems with the most predicted work come first (longest-processing-time
+    first keeps the final tail short).  ``work`` is any per-system estimate of
+    remaining steps (span, or span x measured step rate).  With ``shares``,
+    every bucket starts at once with a fraction of the GPU proportional to its
+    predicted cost (sum of work x cost per step)."""
     K = np.asarray(K)
+    work = np.asarray(work, dtype=np.float64)
     idx_all = np.arange(K.shape[0]) if active is None else np.nonzero(active)[0]
     ks = np.unique(K[idx_all])
     ks = ks[np.argsort(-cost_weight(ks), kind="stable")]
     order: List[np.ndarray] = []
     begins = [0]
+    cost = []
     for k in ks:
         sel = idx_all[K[idx_all] == k]
-        sel = sel[np.argsort(-span[sel], kind="stable")]
+        sel = sel[np.argsort(-work[sel], kind="stable")]
         order.append(sel)
         begins.append(begins[-1] + sel.size)
+        cost.append(float(np.sum(work[sel])) * float(cost_weight(k)[0]))
+    sh = None
+    if shares and len(ks) > 1:
+        c = np.asarray(cost)
+        sh = (c / c.sum()).astype(np.float32) if c.sum() > 0 else None
     return WorkList(order=np.concatenate(order).astype(np.int32) if order else np.zeros(0, np.int32),
-                    bucket_K=ks.astype(np.int32), bucket_begin=np.asarray(begins, dtype=np.int32))
+                    bucket_K=ks.astype(np.int32), bucket_begin=np.asarray(begins, dtype=np.int32), share=sh)
 
 
 class Ensemble:
@@ -135,6 +156,14 @@ class Ensemble:
         self.dev = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in self.host.items()}
         return self
 
+    def enable_trace(self) -> None:
+        """Record per-system load / write-back GPU timestamps (ns) in
+        dev['trace_load_ns'] / dev['trace_done_ns'] on later solves and plans."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        self.dev["trace_load_ns"] = torch.zeros(self.ns, dtype=torch.int64, device=dev)
+        self.dev["trace_done_ns"] = torch.zeros(self.ns, dtype=torch.int64, device=dev)
+
     def reset_device(self) -> None:
         """Copy the host arrays (initial conditions) into the existing device arrays."""
         import torch
@@ -160,6 +189,9 @@ class Ensemble:
                      "control_params", "coupling", "t", "t_end", "t_begin", "h", "event", "status",
                      "steps", "rejected", "conv_ok", "conv_fail", "lin_iters"):
             setattr(e, name, d[name].data_ptr())
+        if "trace_load_ns" in d:
+            e.trace_load_ns = d["trace_load_ns"].data_ptr()
+            e.trace_done_ns = d["trace_done_ns"].data_ptr()
         if self.ndo > 0:
             e.dense_index = d["dense_index"].data_ptr()
             e.dense_time = d["dense_time"].data_ptr()
@@ -189,6 +221,10 @@ class Ensemble:
             bp = np.ascontiguousarray(wl.blocks_per_sm, dtype=np.int32)
             keep.append(bp)
             w.blocks_per_sm = bp.ctypes.data
+        if wl.share is not None:
+            sh = np.ascontiguousarray(wl.share, dtype=np.float32)
+            keep.append(sh)
+            w.share = sh.ctypes.data
         return w, keep
 
     # ---- solving ----
@@ -210,7 +246,7 @@ class Ensemble:
             self.to_device()
         return Plan(self, max_steps, work)
 
-    def scheduled_plan(self, max_steps: int = 1_000_000, pilot_steps: int = 256) -> "ScheduledPlan":
+    def scheduled_plan(self, max_steps: int = 1_000_000, pilot_steps: int = 2048) -> "ScheduledPlan":
         if not self.dev:
             self.to_device()
         return ScheduledPlan(self, max_steps, pilot_steps)
@@ -219,55 +255,58 @@ class Ensemble:
 class ScheduledPlan:
     """Two-phase batched solve with measured longest-first ordering.
 
-    Phase 1 (pilot) advances every system by at most ``pilot_steps`` steps.
-    The step rate it measures predicts each system's remaining work,
-    (t_end - t) * pilot_steps / (t - t_start).  On the device, each K bucket
-    of the phase-2 work list is re-sorted by that prediction (longest first,
-    finished systems last), and phase 2 spends the rest of the budget.  Every
-    call resumes exactly where the previous one stopped, so the results are
-    bit-identical to a single solve with the same total budget; only the
-    order in which warps pick up systems changes, which shortens the tail.
-    ``launch()`` = pilot graph + a few sort kernels + main graph, all on one
-    stream without host synchronisation.
+    Phase 1 (pilot, one graph launch) advances every system by at most
+    ``pilot_steps`` steps.  The step rate it measures predicts each system's
+    remaining steps, (t_end - t) * pilot_steps / (t - t_start).  Phase 2 solves
+    the systems still running with every K bucket started at once, a GPU share
+    per bucket proportional to its predicted cost, and each bucket's systems
+    in longest-predicted-first order.  Every call resumes exactly where the
+    previous one stopped, so the results are bit-identical to a single solve
+    with the same total budget; only the order in which warps pick systems up
+    changes, which shortens the tail.
     """
 
-    def __init__(self, ens: Ensemble, max_steps: int, pilot_steps: int = 256):
-        import torch
+    def __init__(self, ens: Ensemble, max_steps: int, pilot_steps: int = 2048):
         if pilot_steps >= max_steps:
             raise ValueError("pilot_steps must be smaller than max_steps")
         self.ens = ens
+        self.max_steps = int(max_steps)
         self.pilot_steps = int(pilot_steps)
-        wl = make_work_list(ens.host["K"], ens.host["t_end"] - ens.host["t"])
-        self.pilot = Plan(ens, self.pilot_steps, wl)
-        main_wl = WorkList(order=wl.order.copy(), bucket_K=wl.bucket_K, bucket_begin=wl.bucket_begin)
-        self.main = Plan(ens, int(max_steps) - self.pilot_steps, main_wl)
-        dev = torch.device("cuda", ens.device)
-        self.order_dev = self.main._keep[0]          # the main plan's device order array
-        K = ens.host["K"]
-        rank = np.empty(ens.ns, dtype=np.int64)
-        for b, k in enumerate(wl.bucket_K):
-            rank[K == k] = b
-        self.bucket_rank = torch.from_numpy(rank).to(dev)
-        self.t_start = torch.empty(ens.ns, dtype=torch.float64, device=dev)
+        span = ens.host["t_end"] - ens.host["t"]
+        self.pilot = Plan(ens, self.pilot_steps, make_work_list(ens.host["K"], span))
+        self.last_work: Optional[WorkList] = None
+        self.rate_clip = (200.0, 20000.0)   # steps per period
 
     def launch(self, stream=None) -> None:
         import torch
         d = self.ens.dev
-        st = stream if stream is not None else torch.cuda.current_stream(self.ens.device)
-        with torch.cuda.stream(st):
-            self.t_start.copy_(d["t"])
-            self.pilot.launch(st)
-            adv = (d["t"] - self.t_start).clamp(min=1e-300)
-            remaining = (d["t_end"] - d["t"]).clamp(min=0.0) * (self.pilot_steps / adv)
-            remaining = torch.where(d["status"] == -1, remaining, torch.zeros_like(remaining))
-            by_cost = torch.sort(-remaining, stable=True).indices
-            by_bucket = torch.sort(self.bucket_rank[by_cost], stable=True).indices
-            self.order_dev.copy_(by_cost[by_bucket].to(torch.int32))
-            self.main.launch(st)
+        t_start = d["t"].clone()
+        self.pilot.launch(stream)
+        torch.cuda.synchronize(self.ens.device)
+        t = d["t"].cpu().numpy()
+        t0 = t_start.cpu().numpy()
+        status = d["status"].cpu().numpy()
+        t_end = d["t_end"].cpu().numpy()
+        adv = np.maximum(t - t0, 1e-300)
+        # a system caught in a collapse during the pilot advances very little:
+        # clip its measured rate to a plausible range before extrapolating
+        rate = np.clip(self.pilot_steps / adv, self.rate_clip[0], self.rate_clip[1])
+        remaining = np.maximum(t_end - t, 0.0)
+        pred = remaining * rate
+        active = status == -1
+        if not np.any(active):
+            return
+        K = self.ens.host["K"]
+        wl = make_work_list(K, pred, active=active)
+        # bucket shares from the remaining spans (robust); the measured rates
+        # only order the systems inside each bucket
+        span_wl = make_work_list(K, remaining, active=active)
+        wl.share = span_wl.share
+        self.last_work = wl
+        self.ens.solve(self.max_steps - self.pilot_steps, work=wl, stream=stream)
 
     def close(self) -> None:
         self.pilot.close()
-        self.main.close()
 
 
 class Plan:

@@ -77,56 +77,93 @@ static EnsLayout make_layout(const cbc_ensemble* e) {
   E.conv_ok = e->conv_ok;
   E.conv_fail = e->conv_fail;
   E.lin_iters = (long long*)e->lin_iters;
+  E.trace_load_ns = (long long*)e->trace_load_ns;
+  E.trace_done_ns = (long long*)e->trace_done_ns;
   E.up_stride = e->up_stride;
   E.sp_stride = e->sp_stride;
   E.cp_stride = e->cp_stride;
   return E;
 }
 
-// Persistent grid size per bucket: resident blocks per SM (occupancy, or the
-// work list's override if smaller) times the SM count, but never more warps
-// than the bucket has system slots to fill.  Computed before any capture.
-static std::vector<int> grid_sizes(cbc_context* ctx, const cbc_spec* spec, const cbc_work* w) {
-  std::vector<int> out(w->nbuckets, 0);
+// Persistent grid sizes per bucket, computed before any capture.  first[b]
+// blocks start with the launch; second[b] more are launched behind every
+// bucket's first grid (backfill).  A full-GPU grid is the resident blocks per
+// SM (occupancy, or the work list's smaller override) times the SM count; no
+// bucket gets more warps than it has systems to fill.
+// Default block size of the batched kernels (2 warps: finer packing of
+// blocks from different buckets on one SM).
+constexpr int kDefaultThreads = 64;
+constexpr float kStartFill = 0.85f;
+
+struct Grids {
+  std::vector<int> first, second;
+};
+
+static Grids grid_sizes(cbc_context* ctx, const cbc_spec* spec, const cbc_work* w) {
+  Grids g;
+  g.first.assign(w->nbuckets, 0);
+  g.second.assign(w->nbuckets, 0);
   for (int b = 0; b < w->nbuckets; ++b) {
     const int begin = w->bucket_begin[b], end = w->bucket_begin[b + 1];
     if (end <= begin) continue;
     const int K = w->bucket_K[b];
-    const int threads = w->threads ? w->threads[b] : 128;
+    const int threads = w->threads ? w->threads[b] : kDefaultThreads;
     const int per_sm = resident_blocks(K, spec->nk, threads);
-    int blocks = per_sm * ctx->sm_count;
+    int full = per_sm * ctx->sm_count;
     if (w->blocks_per_sm && w->blocks_per_sm[b] > 0 && w->blocks_per_sm[b] < per_sm)
-      blocks = w->blocks_per_sm[b] * ctx->sm_count;
+      full = w->blocks_per_sm[b] * ctx->sm_count;
     const long long warps_needed = ((long long)(end - begin) + (32 / K) - 1) / (32 / K);
     const long long blocks_needed = (warps_needed * 32 + threads - 1) / threads;
-    if (blocks > blocks_needed) blocks = (int)blocks_needed;
-    out[b] = blocks;
+    if (full > blocks_needed) full = (int)blocks_needed;
+    if (w->share) {
+      float sh = w->share[b];
+      if (!(sh > 0.f)) sh = 0.f;
+      if (sh > 1.f) sh = 1.f;
+      // blocks of different buckets pack imperfectly on an SM: start grids
+      // use at most kStartFill of the GPU so that every bucket's fits at once
+      int f = (int)(sh * kStartFill * (float)full + 0.5f);
+      if (f < 1) f = 1;
+      if (f > full) f = full;
+      g.first[b] = f;
+      g.second[b] = full - f;
+    } else {
+      g.first[b] = full;
+    }
   }
-  return out;
+  return g;
 }
 
 // Enqueues the whole batched solve on `stream`: every bucket on its own
 // forked stream (ctx->side[b]), joined back into `stream`.
 static int32_t enqueue(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e, const cbc_work* w,
-                       const std::vector<int>& grids, int64_t max_steps, int* d_head, cudaStream_t stream) {
+                       const Grids& grids, int64_t max_steps, int* d_head, cudaStream_t stream) {
   const EnsLayout E = make_layout(e);
   const Params P = make_params(*spec);
   CBC_CUDA_TRY(ctx, cudaMemsetAsync(d_head, 0, sizeof(int) * w->nbuckets, stream));
   CBC_CUDA_TRY(ctx, cudaEventRecord(ctx->fork, stream));
-  int used = 0;
-  for (int b = 0; b < w->nbuckets; ++b) {
-    const int begin = w->bucket_begin[b], end = w->bucket_begin[b + 1];
-    if (end <= begin) continue;
-    const int K = w->bucket_K[b];
-    const int threads = w->threads ? w->threads[b] : 128;
-    const int blocks = grids[b];
-    cudaStream_t s = ctx->side[used % CBC_SIDE_STREAMS];
-    CBC_CUDA_TRY(ctx, cudaStreamWaitEvent(s, ctx->fork, 0));
-    CBC_CUDA_TRY(ctx, launch_ensemble_bucket(E, P, w->order, begin, end, K, d_head + b, max_steps, blocks,
-                                             threads, s));
-    CBC_CUDA_TRY(ctx, cudaEventRecord(ctx->join[used % CBC_SIDE_STREAMS], s));
-    CBC_CUDA_TRY(ctx, cudaStreamWaitEvent(stream, ctx->join[used % CBC_SIDE_STREAMS], 0));
-    ++used;
+  int used_first = 0, used_second = 0;
+  // pass 0: every bucket's first grid; pass 1: the backfill grids, launched
+  // after all first grids so that they only take SMs other buckets release
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int b = 0; b < w->nbuckets; ++b) {
+      const int begin = w->bucket_begin[b], end = w->bucket_begin[b + 1];
+      if (end <= begin) continue;
+      const int blocks = pass == 0 ? grids.first[b] : grids.second[b];
+      if (blocks <= 0) continue;
+      const int slot = pass == 0 ? used_first : CBC_SIDE_STREAMS / 2 + used_second;
+      if (slot >= (pass == 0 ? CBC_SIDE_STREAMS / 2 : CBC_SIDE_STREAMS))
+        return fail(ctx, CBC_E_UNSUPPORTED, "too many bucket launches");
+      const int K = w->bucket_K[b];
+      const int threads = w->threads ? w->threads[b] : kDefaultThreads;
+      cudaStream_t s = ctx->side[slot];
+      CBC_CUDA_TRY(ctx, cudaStreamWaitEvent(s, ctx->fork, 0));
+      CBC_CUDA_TRY(ctx, launch_ensemble_bucket(E, P, w->order, begin, end, K, d_head + b, max_steps, blocks,
+                                               threads, s));
+      CBC_CUDA_TRY(ctx, cudaEventRecord(ctx->join[slot], s));
+      CBC_CUDA_TRY(ctx, cudaStreamWaitEvent(stream, ctx->join[slot], 0));
+      if (pass == 0) ++used_first;
+      else ++used_second;
+    }
   }
   return CBC_OK;
 }
@@ -145,7 +182,7 @@ int32_t cbc_ensemble_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_ens
   if (rc) return rc;
   if (max_steps < 1) return fail(ctx, CBC_E_INVALID, "max_steps must be >= 1");
   DeviceGuard dg(ctx->device);
-  const std::vector<int> grids = grid_sizes(ctx, spec, w);
+  const Grids grids = grid_sizes(ctx, spec, w);
   return enqueue(ctx, spec, e, w, grids, max_steps, ctx->d_head, (cudaStream_t)stream);
 }
 
@@ -179,7 +216,7 @@ int32_t cbc_env_plan_create(cbc_context* ctx, const cbc_spec* spec, const cbc_en
     delete p;
     return fail(ctx, CBC_E_CUDA, "cudaMalloc: %s", cudaGetErrorString(ce));
   }
-  const std::vector<int> grids = grid_sizes(ctx, spec, w);
+  const Grids grids = grid_sizes(ctx, spec, w);
   cudaStream_t cs = ctx->capture;
   ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (ce != cudaSuccess) {

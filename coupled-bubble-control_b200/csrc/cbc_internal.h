@@ -13,8 +13,8 @@
 #include "../../include/cbc_b200.h"
 #include "ckm1d_core.cuh"
 
-#define CBC_MAX_BUCKETS 64
-#define CBC_SIDE_STREAMS 8
+#define CBC_MAX_BUCKETS 32   // two launches per bucket fit CBC_SIDE_STREAMS
+#define CBC_SIDE_STREAMS 64
 
 struct cbc_context {
   int device = 0;

@@ -36,6 +36,7 @@ template <int KB>
 __device__ __forceinline__ void ens_load(const EnsLayout& E, const Params& P, const Geo& g, int s, LaneState& S,
                                          MView& M, const WarpSmem& W, long long& boff) {
   boff = E.bubble_offset[s];
+  if (g.li == 0 && E.trace_load_ns) E.trace_load_ns[s] = global_ns();
   const long long b = boff + g.li;
   const double2* st = reinterpret_cast<const double2*>(E.state + b * 4);
   const double2 s01 = st[0], s23 = st[1];
@@ -67,6 +68,7 @@ __device__ __forceinline__ void ens_writeback(const EnsLayout& E, const Params& 
   st[0] = make_double2(S.y[0], S.y[1]);
   st[1] = make_double2(S.y[2], S.y[3]);
   if (g.li == 0) {
+    if (E.trace_done_ns) E.trace_done_ns[s] = global_ns();
     E.t[s] = S.t;
     E.h[s] = S.h;
     E.event[s] = S.g_old;

@@ -39,8 +39,16 @@ struct EnsLayout {
   int* conv_ok;
   int* conv_fail;
   long long* lin_iters;
+  long long* trace_load_ns;   // optional: %globaltimer when a slot picked the system up
+  long long* trace_done_ns;   // optional: %globaltimer when its result was written back
   int up_stride, sp_stride, cp_stride;
 };
+
+__device__ __forceinline__ long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return (long long)t;
+}
 
 cudaError_t launch_ensemble_bucket(const EnsLayout& E, const Params& P, const int* order, int begin, int end,
                                    int K, int* head, long long max_steps, int blocks, int threads,

@@ -184,9 +184,14 @@ int32_t cbc_create(cbc_context** out, int32_t device) {
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming);
+  int prio_low = 0, prio_high = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   for (int i = 0; i < CBC_SIDE_STREAMS && e == cudaSuccess; ++i) {
     e = cudaEventCreateWithFlags(&ctx->join[i], cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking);
+    // first half: higher priority (bucket start grids); second half: lowest
+    // priority (backfill grids only take SMs no start grid is waiting for)
+    const int prio = i < CBC_SIDE_STREAMS / 2 ? prio_high : prio_low;
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ctx->side[i], cudaStreamNonBlocking, prio);
   }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->capture, cudaStreamNonBlocking);
   cudaSetDevice(prev);

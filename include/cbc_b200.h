@@ -183,12 +183,19 @@ typedef struct cbc_ensemble {
   int32_t* conv_ok;
   int32_t* conv_fail;
   int64_t* lin_iters;
+  int64_t* trace_load_ns;  /* optional (ns) i64: GPU global timer when a slot picked the system up */
+  int64_t* trace_done_ns;  /* optional (ns) i64: GPU global timer when its result was written back */
 } cbc_ensemble;
 
 /* Work list: system ids grouped in buckets of equal K (device array `order`),
  * each bucket ordered longest expected work first.  bucket_K, bucket_begin
  * (nbuckets + 1 entries), and the optional tuning arrays threads (per-block
- * threads, 32..128) and blocks_per_sm are host arrays. */
+ * threads, 32..128), blocks_per_sm and share are host arrays.
+ * share[b] (0..1], optional: the bucket's fraction of the GPU at the start.
+ * With shares, every bucket starts at once with share[b] of a full-GPU grid;
+ * the rest of each bucket's grid is launched behind all of them and fills SMs
+ * as other buckets drain.  Without shares each bucket gets a full-GPU grid
+ * and the buckets overlap only at their tails. */
 typedef struct cbc_work {
   const int32_t* order;
   int32_t nbuckets;
@@ -196,6 +203,7 @@ typedef struct cbc_work {
   const int32_t* bucket_begin;
   const int32_t* threads;
   const int32_t* blocks_per_sm;
+  const float* share;
 } cbc_work;
 
 typedef struct cbc_plan cbc_plan;

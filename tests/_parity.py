@@ -58,3 +58,25 @@ def assert_bit_exact(gpu, ref, keys=COMPARED):
 
 def max_rel_err(a, b, floor):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor))) if a.size else 0.0
+
+
+def ensemble_uniform_to_ref(h, K, nk):
+    """Reference-layout host buffers (tile = K) from the ragged arrays of a
+    uniform-K ensemble, for running the oracle on ensemble state."""
+    ns = h["t"].shape[0]
+    st = h["state"].reshape(ns, K, 4)
+    up = h["unit_params"].reshape(ns, K, -1)[:, :, :13]
+    cm = h["coupling"].reshape(ns, 3, K, K)
+    return {
+        "actual_time": h["t"].copy(), "time_end": h["t_end"].copy(), "time_begin": h["t_begin"].copy(),
+        "time_step": h["h"].copy(), "actual_state": np.ascontiguousarray(np.transpose(st, (2, 0, 1))),
+        "unit_params": np.ascontiguousarray(np.transpose(up, (2, 0, 1))),
+        "system_params": np.ascontiguousarray(h["system_params"][:, :5].T),
+        "control_params": np.ascontiguousarray(h["control_params"][:, :4 * nk].T),
+        "coupling_matrices": np.ascontiguousarray(np.transpose(cm, (1, 2, 0, 3))),
+        "dense_index": np.zeros(ns, np.int32), "dense_time": np.zeros((0, ns)),
+        "dense_state": np.zeros((0, 4, ns, K)), "actual_event": h["event"].copy(),
+        "status_flags": h["status"].copy(), "total_steps": np.zeros(ns, np.int32),
+        "rejected_steps": np.zeros(ns, np.int32), "convergece_success": np.zeros(ns, np.int32),
+        "convergence_failures": np.zeros(ns, np.int32), "lin_iters": np.zeros(ns, np.int64),
+    }
