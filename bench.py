@@ -196,12 +196,22 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def make_plan(ens, schedule: str):
+    """adaptive: time slices with re-planning and latency lanes; pilot: one
+    measured re-ordering after a short pilot pass; span: longest span first."""
+    if schedule == "adaptive":
+        return ens.adaptive_plan(MAX_STEPS)
+    if schedule == "pilot":
+        return ens.scheduled_plan(MAX_STEPS, pilot_steps=256)
+    return ens.plan(MAX_STEPS)
+
+
 def batched_once(scene, dev_index: int, schedule: str) -> float:
     """System-periods/s of one batched solve of `scene` (for the ratio)."""
     import torch
     from cbc_b200.ensemble import Ensemble
     ens = Ensemble.from_scene(scene, device=dev_index).to_device()
-    plan = ens.scheduled_plan(MAX_STEPS, 256) if schedule == "pilot" else ens.plan(MAX_STEPS)
+    plan = make_plan(ens, schedule)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     plan.launch()
@@ -278,7 +288,7 @@ def run_b200(args):
     scene = scenes.mixed_k(ns=args.ns, seed=rank_seed(rank))
     ens = Ensemble.from_scene(scene, device=local)
     ens.to_device()
-    plan = ens.scheduled_plan(MAX_STEPS, pilot_steps=256) if args.schedule == "pilot" else ens.plan(MAX_STEPS)
+    plan = make_plan(ens, args.schedule)
     nbuckets = int(np.unique(scene.K).size)
     # pristine device copy of the initial state for the per-step reset
     pristine = {k: v.clone() for k, v in ens.dev.items()}
@@ -297,6 +307,8 @@ def run_b200(args):
         pg.barrier()
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ctx = _lib.default_context(local)
+    launches0 = _lib.lib().cbc_kernel_launches(ctx.handle)
     with ClockSampler(local) as clk:
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
@@ -310,6 +322,7 @@ def run_b200(args):
         torch.cuda.synchronize()
     if pg:
         pg.barrier()
+    launches = _lib.lib().cbc_kernel_launches(ctx.handle) - launches0
     total_ms = t0.elapsed_time(t1)
     kern_ms = [a.elapsed_time(b) for a, b in ev]
     res = ens.to_host()
@@ -382,7 +395,7 @@ def run_b200(args):
                          "note": "algorithmic FP64 flops (transcendentals counted as 1) / graph time; "
                                  "peak = cuBLAS FP64 GEMM measured in this run"},
             "clocks": clk.summary(),
-            "gpu_launches": args.steps * nbuckets * (2 if args.schedule == "pilot" else 1),
+            "gpu_launches": int(launches),
         }
         if plain:
             line["plain"] = plain
@@ -413,7 +426,7 @@ def main():
     ap.add_argument("--no-env", dest="env", action="store_false")
     ap.add_argument("--plain-ns", type=int, default=16384, help="systems used for the batched-vs-plain ratio")
     ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--schedule", default="pilot", choices=["pilot", "span"],
+    ap.add_argument("--schedule", default="adaptive", choices=["adaptive", "pilot", "span"],
                     help="pilot: measured longest-first re-ordering after a pilot pass; span: longest span first")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -56,7 +56,8 @@ class cbc_ensemble(ctypes.Structure):
 
 class cbc_work(ctypes.Structure):
     _fields_ = [("order", P), ("nbuckets", i32), ("bucket_K", P), ("bucket_begin", P), ("threads", P),
-                ("blocks_per_sm", P), ("share", P)]
+                ("blocks_per_sm", P), ("share", P), ("exclusive", P), ("budget_ns", i64),
+                ("steps_total", i32), ("reserved", i32)]
 
 
 class cbc_env_io(ctypes.Structure):
@@ -119,6 +120,7 @@ EXTRA_SIGNATURES: list = [
     ("cbc_env_plan_create", i32, [P, ctypes.POINTER(cbc_spec), ctypes.POINTER(cbc_ensemble),
                                   ctypes.POINTER(cbc_work), i64, ctypes.POINTER(cbc_env_io), ctypes.POINTER(P)]),
     ("cbc_plan_launch", i32, [P, P]),
+    ("cbc_kernel_launches", i64, [P]),
     ("cbc_plan_destroy", i32, [P]),
 ]
 

@@ -34,11 +34,15 @@ class WorkList:
     threads: Optional[np.ndarray] = None
     blocks_per_sm: Optional[np.ndarray] = None
     share: Optional[np.ndarray] = None   # (nb,) float32 fraction of the GPU per bucket at the start
+    exclusive: Optional[np.ndarray] = None   # (nb,) int32 SMs of a latency lane (0: ordinary bucket)
 
 
-# Steady-state cost of one system-step on a full B200 (ns), measured on
-# ensembles of identical systems (no tail); other K are interpolated.
-STEP_NS = {1: 0.6, 2: 0.995, 3: 2.65, 4: 3.13, 6: 9.24, 8: 12.6}
+# Steady-state cost of one step attempt on a full B200 (ns), measured on
+# uniform-K ensembles with every slot busy (no tail); other K are interpolated.
+STEP_NS = {1: 0.55, 2: 0.80, 3: 2.09, 4: 2.57, 6: 7.50, 8: 10.35}
+# Latency of one step attempt of a system whose warp has an SM sub-partition
+# to itself (us), measured on single systems of the mixed-K workload.
+ALONE_US = {1: 18.0, 2: 20.8, 3: 23.0, 4: 26.0, 6: 31.0, 8: 35.5}
 
 
 def cost_weight(K) -> np.ndarray:
@@ -49,6 +53,18 @@ def cost_weight(K) -> np.ndarray:
     out = np.interp(K, ks, vs)
     big = K > ks[-1]
     out[big] = vs[-1] * (K[big] / ks[-1]) ** 2
+    return out
+
+
+def alone_latency(K) -> np.ndarray:
+    """Per-attempt latency (us) of a K-bubble system running alone on an SM
+    sub-partition; K > 8 extrapolated linearly in K."""
+    K = np.atleast_1d(np.asarray(K, dtype=np.float64))
+    ks = np.asarray(sorted(ALONE_US), dtype=np.float64)
+    vs = np.asarray([ALONE_US[int(k)] for k in ks])
+    out = np.interp(K, ks, vs)
+    big = K > ks[-1]
+    out[big] = vs[-1] * K[big] / ks[-1]
     return out
 
 
@@ -80,6 +96,65 @@ def make_work_list(K: np.ndarray, work: np.ndarray, active: Optional[np.ndarray]
         sh = (c / c.sum()).astype(np.float32) if c.sum() > 0 else None
     return WorkList(order=np.concatenate(order).astype(np.int32) if order else np.zeros(0, np.int32),
                     bucket_K=ks.astype(np.int32), bucket_begin=np.asarray(begins, dtype=np.int32), share=sh)
+
+
+def with_latency_lane(wl: WorkList, K: np.ndarray, work: np.ndarray, fraction: float = 1e-3,
+                      max_sms: int = 12) -> WorkList:
+    """Moves the systems with the longest predicted serial time into latency
+    lanes: extra buckets of the same K whose blocks (4 warps) each hold an SM
+    alone, so their steps run at the minimum latency instead of sharing issue
+    slots with a full SM.  The serial time of a system is its predicted steps
+    times the per-step latency of its warp on a full GPU, which grows with the
+    cost of one system-step and the number of systems a warp carries.  At most
+    ``fraction`` of the systems and ``max_sms`` SMs are used."""
+    K = np.asarray(K)
+    work = np.asarray(work, dtype=np.float64)
+    if wl.order.size == 0 or max_sms < 1:
+        return wl
+    ids = wl.order
+    chain = work[ids] * cost_weight(K[ids]) * (32 // K[ids])
+    n_lat = int(np.ceil(fraction * ids.size))
+    top = ids[np.argsort(-chain, kind="stable")[:n_lat]]
+    # trim to the SM budget, keeping the longest chains
+    picked, count, sms = [], {}, {}
+    used = 0
+    for s_ in top:
+        k = int(K[s_])
+        opens_block = count.get(k, 0) % (4 * (32 // k)) == 0   # a new 4-warp block, one more SM
+        if opens_block and used + 1 > max_sms:
+            continue
+        if opens_block:
+            sms[k] = sms.get(k, 0) + 1
+            used += 1
+        count[k] = count.get(k, 0) + 1
+        picked.append(int(s_))
+    if not picked:
+        return wl
+    order, bk, bb = [], [], [0]
+    share = [] if wl.share is not None else None
+    excl = []
+    for b in range(wl.bucket_K.size):
+        seg = wl.order[wl.bucket_begin[b]:wl.bucket_begin[b + 1]]
+        seg = seg[~np.isin(seg, picked)]
+        order.append(seg)
+        bk.append(int(wl.bucket_K[b]))
+        bb.append(bb[-1] + seg.size)
+        excl.append(0)
+        if share is not None:
+            share.append(float(wl.share[b]))
+    for k in sorted(sms, key=lambda k: -cost_weight(k)[0]):
+        sel = np.asarray([p for p in picked if int(K[p]) == k], dtype=np.int32)
+        sel = sel[np.argsort(-work[sel], kind="stable")]
+        order.append(sel)
+        bk.append(k)
+        bb.append(bb[-1] + sel.size)
+        excl.append(sms[k])
+        if share is not None:
+            share.append(0.0)
+    return WorkList(order=np.concatenate(order).astype(np.int32), bucket_K=np.asarray(bk, np.int32),
+                    bucket_begin=np.asarray(bb, np.int32), threads=None, blocks_per_sm=None,
+                    share=None if share is None else np.asarray(share, np.float32),
+                    exclusive=np.asarray(excl, np.int32))
 
 
 class Ensemble:
@@ -198,7 +273,7 @@ class Ensemble:
             e.dense_state = d["dense_state"].data_ptr()
         return e
 
-    def work(self, wl: Optional[WorkList] = None):
+    def work(self, wl: Optional[WorkList] = None, budget_ns: int = 0, steps_total: bool = False):
         """(cbc_work, keep-alive list) for a work list (default: all systems)."""
         import torch
         if wl is None:
@@ -225,17 +300,27 @@ class Ensemble:
             sh = np.ascontiguousarray(wl.share, dtype=np.float32)
             keep.append(sh)
             w.share = sh.ctypes.data
+        if wl.exclusive is not None:
+            ex = np.ascontiguousarray(wl.exclusive, dtype=np.int32)
+            keep.append(ex)
+            w.exclusive = ex.ctypes.data
+        w.budget_ns = int(budget_ns)
+        w.steps_total = 1 if steps_total else 0
         return w, keep
 
     # ---- solving ----
-    def solve(self, max_steps: int = 1_000_000, work: Optional[WorkList] = None, stream=None) -> None:
-        """Enqueue one batched solve on `stream` (default: current torch stream)."""
+    def solve(self, max_steps: int = 1_000_000, work: Optional[WorkList] = None, stream=None,
+              budget_ns: int = 0, steps_total: bool = False) -> None:
+        """Enqueue one batched solve on `stream` (default: current torch stream).
+        budget_ns > 0 stops every system that long after the solve starts
+        (resumable, status -1); steps_total makes max_steps a cap on the steps
+        accumulated over all calls."""
         import torch
         if not self.dev:
             self.to_device()
         ctx = _lib.default_context(self.device)
         spec, e = self.spec(), self.abi()
-        w, keep = self.work(work)
+        w, keep = self.work(work, budget_ns, steps_total)
         st = stream if stream is not None else torch.cuda.current_stream(self.device)
         ctx.check(_lib.lib().cbc_ensemble_solve(ctx.handle, ctypes.byref(spec), ctypes.byref(e),
                                                 ctypes.byref(w), int(max_steps), ctypes.c_void_p(st.cuda_stream)))
@@ -246,10 +331,17 @@ class Ensemble:
             self.to_device()
         return Plan(self, max_steps, work)
 
-    def scheduled_plan(self, max_steps: int = 1_000_000, pilot_steps: int = 2048) -> "ScheduledPlan":
+    def adaptive_plan(self, max_steps: int = 1_000_000, slices=(1.0, 2.0, 4.0, 8.0),
+                      max_lane_sms: int = 24) -> "AdaptivePlan":
         if not self.dev:
             self.to_device()
-        return ScheduledPlan(self, max_steps, pilot_steps)
+        return AdaptivePlan(self, max_steps, slices, max_lane_sms)
+
+    def scheduled_plan(self, max_steps: int = 1_000_000, pilot_steps: int = 2048,
+                       latency_lane: bool = True) -> "ScheduledPlan":
+        if not self.dev:
+            self.to_device()
+        return ScheduledPlan(self, max_steps, pilot_steps, latency_lane)
 
 
 class ScheduledPlan:
@@ -260,13 +352,14 @@ class ScheduledPlan:
     remaining steps, (t_end - t) * pilot_steps / (t - t_start).  Phase 2 solves
     the systems still running with every K bucket started at once, a GPU share
     per bucket proportional to its predicted cost, and each bucket's systems
-    in longest-predicted-first order.  Every call resumes exactly where the
+    in longest-predicted-first order; the systems with the longest predicted
+    serial time run in latency lanes (``with_latency_lane``).  Every call resumes exactly where the
     previous one stopped, so the results are bit-identical to a single solve
     with the same total budget; only the order in which warps pick systems up
     changes, which shortens the tail.
     """
 
-    def __init__(self, ens: Ensemble, max_steps: int, pilot_steps: int = 2048):
+    def __init__(self, ens: Ensemble, max_steps: int, pilot_steps: int = 2048, latency_lane: bool = True):
         if pilot_steps >= max_steps:
             raise ValueError("pilot_steps must be smaller than max_steps")
         self.ens = ens
@@ -276,6 +369,7 @@ class ScheduledPlan:
         self.pilot = Plan(ens, self.pilot_steps, make_work_list(ens.host["K"], span))
         self.last_work: Optional[WorkList] = None
         self.rate_clip = (200.0, 20000.0)   # steps per period
+        self.latency_lane = bool(latency_lane)
 
     def launch(self, stream=None) -> None:
         import torch
@@ -302,11 +396,153 @@ class ScheduledPlan:
         # only order the systems inside each bucket
         span_wl = make_work_list(K, remaining, active=active)
         wl.share = span_wl.share
+        if self.latency_lane:
+            wl = with_latency_lane(wl, K, pred)
         self.last_work = wl
         self.ens.solve(self.max_steps - self.pilot_steps, work=wl, stream=stream)
 
     def close(self) -> None:
         self.pilot.close()
+
+
+def lane_work_list(wl: WorkList, K: np.ndarray, lane_ids: np.ndarray, order_key: np.ndarray,
+                   sms_by_k: Dict[int, int]) -> WorkList:
+    """Moves the systems lane_ids out of the buckets of wl into latency lanes:
+    one extra bucket per K with sms_by_k[K] exclusive SMs, longest order_key
+    first."""
+    lane_ids = np.asarray(lane_ids)
+    order, bk, bb = [], [], [0]
+    share = [] if wl.share is not None else None
+    excl = []
+    for b in range(wl.bucket_K.size):
+        seg = wl.order[wl.bucket_begin[b]:wl.bucket_begin[b + 1]]
+        seg = seg[~np.isin(seg, lane_ids)]
+        order.append(seg)
+        bk.append(int(wl.bucket_K[b]))
+        bb.append(bb[-1] + seg.size)
+        excl.append(0)
+        if share is not None:
+            share.append(float(wl.share[b]))
+    for k in sorted(sms_by_k, key=lambda k: -cost_weight(k)[0]):
+        sel = lane_ids[K[lane_ids] == k]
+        if sel.size == 0 or sms_by_k[k] < 1:
+            continue
+        sel = sel[np.argsort(-order_key[sel], kind="stable")]
+        order.append(sel)
+        bk.append(int(k))
+        bb.append(bb[-1] + sel.size)
+        excl.append(int(sms_by_k[k]))
+        if share is not None:
+            share.append(0.0)
+    return WorkList(order=np.concatenate(order).astype(np.int32), bucket_K=np.asarray(bk, np.int32),
+                    bucket_begin=np.asarray(bb, np.int32),
+                    share=None if share is None else np.asarray(share, np.float32),
+                    exclusive=np.asarray(excl, np.int32))
+
+
+class AdaptivePlan:
+    """Time-sliced batched solve that re-plans between slices.
+
+    Which systems run longest cannot be told from their first steps: in the
+    mixed-K workload a third of the K = 8 systems fail early (step-size
+    limit, non-convergence, non-finite state) after stepping just as fast as
+    the systems that run to the end.  Long systems reveal themselves by
+    surviving.  So the solve runs in slices of device time (``slices``
+    seconds, then one unbounded slice); every slice stops all systems after
+    their current step (resumable, bit-identical), and the host re-plans the
+    rest from the progress seen so far:
+
+    * remaining attempts of a system = its observed attempts per unit of
+      simulated time x its remaining span (the median rate of its K while it
+      has not run enough steps to measure its own);
+    * a system whose remaining attempts at its alone latency (``ALONE_US``)
+      exceed the predicted bulk time would end last: it goes to a latency
+      lane (an SM of its own, ``cbc_work.exclusive``), longest first, up to
+      ``max_lane_sms`` SMs;
+    * every other system goes to its K bucket, longest first, with bucket
+      shares proportional to the predicted cost (``STEP_NS``).
+
+    max_steps caps the steps each system accumulates over all slices
+    (``steps_total``), so the results equal one solve with that cap.
+    """
+
+    MIN_OBSERVED = 256   # attempts before a system's own rate is trusted
+
+    def __init__(self, ens: Ensemble, max_steps: int, slices=(1.0, 2.0, 4.0, 8.0), max_lane_sms: int = 24):
+        self.ens = ens
+        self.max_steps = int(max_steps)
+        self.slices = [float(s) for s in slices]
+        self.max_lane_sms = int(max_lane_sms)
+        self.history: List[dict] = []
+        import torch
+        self.sm_count = torch.cuda.get_device_properties(ens.device).multi_processor_count
+
+    def plan(self, K, t_end, t0, a0, t, attempts, active) -> WorkList:
+        ids = np.nonzero(active)[0]
+        adv = t - t0
+        obs = attempts - a0
+        own = (obs >= self.MIN_OBSERVED) & (adv > 0)
+        rate = np.zeros(K.shape[0])
+        rate[own] = obs[own] / adv[own]
+        for k in np.unique(K[ids]):
+            sel = (K == k) & own
+            fill = float(np.median(rate[sel])) if np.any(sel) else 2000.0
+            rate[(K == k) & ~own] = fill
+        remaining = rate * np.maximum(t_end - t, 0.0)
+        serial_s = remaining * alone_latency(K) * 1e-6
+        bulk_s = float(np.sum(remaining[ids] * cost_weight(K[ids]))) * 1e-9
+        wl = make_work_list(K, remaining, active=active)
+        # latency lanes for the systems that would otherwise end last
+        lane_sms = 0
+        picked: List[int] = []
+        sms: Dict[int, int] = {}
+        count: Dict[int, int] = {}
+        for s in ids[np.argsort(-serial_s[ids], kind="stable")]:
+            rest = self.sm_count - lane_sms
+            if serial_s[s] * 1.1 < bulk_s * self.sm_count / max(rest, 1):
+                break
+            k = int(K[s])
+            opens = count.get(k, 0) % (4 * (32 // k)) == 0
+            if opens and lane_sms + 1 > self.max_lane_sms:
+                break
+            if opens:
+                sms[k] = sms.get(k, 0) + 1
+                lane_sms += 1
+            count[k] = count.get(k, 0) + 1
+            picked.append(int(s))
+        if picked:
+            wl = lane_work_list(wl, K, np.asarray(picked), serial_s, sms)
+        self.history.append({"active": int(ids.size), "bulk_s": bulk_s, "lane_systems": len(picked),
+                             "lane_sms": lane_sms, "max_serial_s": float(serial_s[ids].max()) if ids.size else 0.0})
+        return wl
+
+    def launch(self, stream=None) -> None:
+        import torch
+        ens, d = self.ens, self.ens.dev
+        K = ens.host["K"]
+        t_end = d["t_end"].cpu().numpy()
+        t0 = d["t"].cpu().numpy()
+        a0 = (d["steps"] + d["rejected"]).cpu().numpy().astype(np.int64)
+        self.history = []
+        for sl in self.slices + [0.0]:
+            t = d["t"].cpu().numpy()
+            status = d["status"].cpu().numpy()
+            steps = d["steps"].cpu().numpy()
+            attempts = steps.astype(np.int64) + d["rejected"].cpu().numpy()
+            active = ((status == _lib.ACTIVE) | (status == _lib.MAX_STEPS_REACHED)) & (steps < self.max_steps)
+            if not np.any(active):
+                break
+            wl = self.plan(K, t_end, t0, a0, t, attempts, active)
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
+            ens.solve(self.max_steps, work=wl, stream=stream, budget_ns=int(sl * 1e9), steps_total=True)
+            ev[1].record()
+            torch.cuda.synchronize(ens.device)
+            self.history[-1].update(slice_s=sl, device_s=ev[0].elapsed_time(ev[1]) * 1e-3,
+                                    attempts_before=int(attempts.sum() - a0.sum()))
+
+    def close(self) -> None:
+        pass
 
 
 class Plan:

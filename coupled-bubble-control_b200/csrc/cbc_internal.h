@@ -11,6 +11,8 @@
 #include <string>
 
 #include "../../include/cbc_b200.h"
+
+#include <type_traits>
 #include "ckm1d_core.cuh"
 
 #define CBC_MAX_BUCKETS 32   // two launches per bucket fit CBC_SIDE_STREAMS
@@ -27,6 +29,7 @@ struct cbc_context {
   cudaEvent_t join[CBC_SIDE_STREAMS] = {};
   cudaStream_t side[CBC_SIDE_STREAMS] = {};
   cudaStream_t capture = nullptr;  // stream used to capture plans into graphs
+  long long launches = 0;          // kernels enqueued (plans: per replay)
   std::string err;
 };
 
@@ -112,6 +115,11 @@ inline int32_t check_spec(cbc_context* ctx, const cbc_spec* s) {
   return CBC_OK;
 }
 
+// Scheduling scratch of one batched solve: the work-list cursors (one int per
+// bucket) followed by the epoch word (device clock at the solve's start).
+constexpr size_t kHeadBytes = sizeof(int) * CBC_MAX_BUCKETS;
+constexpr size_t kScheduleBytes = kHeadBytes + 2 * sizeof(long long);
+
 // Smallest power-of-two instantiation that holds K bubbles per system.
 inline int kb_for(int K) {
   if (K <= 2) return 2;
@@ -119,6 +127,30 @@ inline int kb_for(int K) {
   if (K <= 8) return 8;
   if (K <= 16) return 16;
   return 32;
+}
+
+// Calls f(KB, KC) with std::integral_constant arguments: KB the power-of-two
+// lanes per system slot, KC the exact K when it is compiled in (K <= 8: the
+// group geometry, partner loops and reductions fold to constants), else 0
+// (K read at run time).
+template <int V>
+using IC = std::integral_constant<int, V>;
+
+template <class F>
+decltype(auto) dispatch_k(int K, F&& f) {
+  switch (K) {
+    case 1: return f(IC<2>{}, IC<1>{});
+    case 2: return f(IC<2>{}, IC<2>{});
+    case 3: return f(IC<4>{}, IC<3>{});
+    case 4: return f(IC<4>{}, IC<4>{});
+    case 5: return f(IC<8>{}, IC<5>{});
+    case 6: return f(IC<8>{}, IC<6>{});
+    case 7: return f(IC<8>{}, IC<7>{});
+    case 8: return f(IC<8>{}, IC<8>{});
+    default:
+      if (K <= 16) return f(IC<16>{}, IC<0>{});
+      return f(IC<32>{}, IC<0>{});
+  }
 }
 
 }  // namespace cbc

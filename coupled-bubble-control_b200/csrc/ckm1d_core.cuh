@@ -122,23 +122,50 @@ __device__ __forceinline__ int partner_lane(const Geo& g, int d) {
   return g.base + j;
 }
 
+// The same for shared-memory exchange records: lanes outside every group read
+// their own record (always inside the warp's 32 records).
+__device__ __forceinline__ int partner_rec(const Geo& g, int d) { return g.valid ? partner_lane(g, d) : g.lane; }
+
+// Open pairwise tree over a[0..n-1] (n <= N): at width w, a[i] += a[i + w]
+// for i a multiple of 2w with i + w < n; a lone last element is carried up.
+// ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + a6).  0.0 for n = 0.  For
+// non-negative terms it equals the zero-padded tree of group_sum.
+template <int N>
+__device__ __forceinline__ double tree_open(double (&a)[N], int n) {
+#pragma unroll
+  for (int w = 1; w < N; w <<= 1) {
+#pragma unroll
+    for (int i = 0; i + w < N; i += 2 * w)
+      if (i + w < n) a[i] = a[i] + a[i + w];
+  }
+  return n > 0 ? a[0] : 0.0;
+}
+
 // Per-warp shared-memory carve-up, in doubles.
 struct WarpSmem {
   double* hc;   // [7 nk][G]   harmonic constants of each group (component-major)
   double* up;   // [15][32]    bubble constants, lane-private columns
   double* ks;   // [6][4][32]  stage derivatives, lane-private columns
+  double* xv;   // [2][32] double2 partner-state exchange records
 };
 
+constexpr int XV_DOUBLES = 4 * 32;
+
+// Harmonic-constant region rounded up to an even count, so that every later
+// region (and every warp's carve-up) stays 16-byte aligned for double2 access.
+__host__ __device__ inline int hc_doubles(int K, int nk) { return (HC_PER_K * nk * (32 / K) + 1) & ~1; }
+
 __host__ __device__ inline int smem_doubles_per_warp(int K, int nk) {
-  return HC_PER_K * nk * (32 / K) + NUPS * 32 + 24 * 32;
+  return hc_doubles(K, nk) + NUPS * 32 + 24 * 32 + XV_DOUBLES;
 }
 
 __device__ __forceinline__ WarpSmem warp_smem(double* base, int K, int nk) {
   WarpSmem w;
   double* p = base + (threadIdx.x >> 5) * smem_doubles_per_warp(K, nk);
   w.hc = p;
-  w.up = p + HC_PER_K * nk * (32 / K);
+  w.up = p + hc_doubles(K, nk);
   w.ks = w.up + NUPS * 32;
+  w.xv = w.ks + 24 * 32;
   return w;
 }
 
@@ -262,6 +289,40 @@ __device__ __forceinline__ double group_event(const double y[4], double up12, co
 
 // RHS of the whole system, evaluated by its K lanes: dy of this lane's bubble.
 // Returns via conv/iters the outcome of the implicit-coupling iteration.
+// Group sum with butterfly shuffles, for groups of exactly KB lanes (KB a
+// power of two, groups aligned to KB): the same pairwise tree as group_sum.
+template <int KB>
+__device__ __forceinline__ double group_sum_full(double v) {
+#pragma unroll
+  for (int w = 1; w < KB; w <<= 1) v = v + __shfl_xor_sync(FULL, v, w);
+  return v;
+}
+
+// Residual r = b - A v of the implicit coupling system for this lane's bubble,
+// A = I + off-diagonal partner blocks.  Partner distance d = 1..K-1 goes to
+// accumulation chain (d - 1) mod 4 (increasing d within a chain); the chains
+// are then combined by the open pairwise tree.
+template <int KB>
+__device__ __forceinline__ void residual(const Geo& g, const double* Am, const double* Bm, const double* Cm,
+                                         const double* Dm, double cpf0, double b0, double b1, double vr,
+                                         double vt, double& r0, double& r1) {
+  double ar[4] = {0.0, 0.0, 0.0, 0.0}, at[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int d = 1; d < KB; ++d)
+    if (d < g.K) {
+      const int src = partner_lane(g, d);
+      const double vrj = shfl(vr, src), vtj = shfl(vt, src);
+      const int c = (d - 1) & 3;
+      ar[c] = fma(Am[d], vrj, fma(Bm[d], vtj, ar[c]));
+      at[c] = fma(Cm[d], vrj, fma(Dm[d], vtj, at[c]));
+    }
+  const int nc = g.K - 1 < 4 ? g.K - 1 : 4;
+  const double sr = tree_open(ar, nc);
+  const double st = tree_open(at, nc);
+  r0 = b0 - fma(sr, cpf0, vr);
+  r1 = b1 - (st + vt);
+}
+
 template <int KB>
 __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSmem& W, const MView& M,
                                     double sp0, double sp3, bool on, double t, const double y[4],
@@ -342,14 +403,21 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
   // ---- explicit coupling + matrix of the implicit system over partners ----
   double g0 = 0.0, g1 = 0.0, tn = 0.0, tg2 = 0.0, tg3 = 0.0;
   double Am[KB], Bm[KB], Cm[KB], Dm[KB];
+  // partner states through the exchange records
+  double2* xv2 = reinterpret_cast<double2*>(W.xv);
+  __syncwarp();
+  xv2[g.lane] = make_double2(x0, x1);
+  xv2[32 + g.lane] = make_double2(x2, x3);
+  __syncwarp();
 #pragma unroll
   for (int d = 1; d < KB; ++d) {
     Am[d] = 0.0; Bm[d] = 0.0; Cm[d] = 0.0; Dm[d] = 0.0;
     if (d < K) {
-      const int src = partner_lane(g, d);
+      const int src = partner_rec(g, d);
       // partner state; its coupling terms are recomputed exactly as the
-      // owning lane computes them (cheaper than shuffling seven terms)
-      const double xj0 = shfl(x0, src), xj1 = shfl(x1, src), xj2 = shfl(x2, src), xj3 = shfl(x3, src);
+      // owning lane computes them (cheaper than exchanging seven terms)
+      const double2 xa = xv2[src], xb = xv2[32 + src];
+      const double xj0 = xa.x, xj1 = xa.y, xj2 = xb.x, xj3 = xb.y;
       if (on) {
         const int j = src - g.base;
         const double j02 = xj0 * xj0;
@@ -393,33 +461,37 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
   const double rt = P.lin_rtol2 * bn;
   const double tol2 = rt > P.lin_atol2 ? rt : P.lin_atol2;
   double vr = b0, vt = b1;
-  conv = !on;
+  // The iterate is advanced unconditionally and the answer kept aside, so
+  // that the convergence test (group norm, compare) is off the dependency
+  // chain of the iteration and has no branch; the count and the returned
+  // iterate are those of the plain loop (test, then update): the first
+  // iterate whose residual norm is below tol2, else the one after
+  // lin_max_iter updates.
+  bool found = !on;
+  double ans_r = vr, ans_t = vt;
   iters = 0;
+  const bool full_groups = (g.K == KB);
+  double r0, r1;
+  residual<KB>(g, Am, Bm, Cm, Dm, cpf0, b0, b1, vr, vt, r0, r1);
   for (int it = 0; it < P.lin_max_iter; ++it) {
-    if (__all_sync(FULL, conv)) break;
-    double ar = 0.0, at = 0.0;
-#pragma unroll
-    for (int d = 1; d < KB; ++d)
-      if (d < K) {
-        const int src = partner_lane(g, d);
-        const double vrj = shfl(vr, src), vtj = shfl(vt, src);
-        ar = fma(Am[d], vrj, fma(Bm[d], vtj, ar));
-        at = fma(Cm[d], vrj, fma(Dm[d], vtj, at));
-      }
-    const double ax0 = fma(ar, cpf0, vr);
-    const double ax1 = at + vt;
-    const double r0 = b0 - ax0;
-    const double r1 = b1 - ax1;
-    const double rn = group_sum<KB>(fma(r0, r0, r1 * r1), g);
-    if (!conv) {
-      ++iters;
-      if (rn < tol2) {
-        conv = true;
-      } else {
-        vr = fma(P.omega, r0, vr);
-        vt = fma(P.omega, r1, vt);
-      }
-    }
+    if (__all_sync(FULL, found)) break;
+    const double rr = fma(r0, r0, r1 * r1);
+    double rn;
+    if (full_groups) rn = group_sum_full<KB>(rr);
+    else rn = group_sum<KB>(rr, g);
+    const bool hit = !found & (rn < tol2);
+    iters = found ? iters : it + 1;
+    ans_r = hit ? vr : ans_r;
+    ans_t = hit ? vt : ans_t;
+    found = found | hit;
+    vr = fma(P.omega, r0, vr);
+    vt = fma(P.omega, r1, vt);
+    residual<KB>(g, Am, Bm, Cm, Dm, cpf0, b0, b1, vr, vt, r0, r1);
+  }
+  conv = found;
+  if (found) {
+    vr = ans_r;
+    vt = ans_t;
   }
   if (!on) conv = true;
   dy[0] = x2;

@@ -84,13 +84,14 @@ __device__ __forceinline__ void ens_writeback(const EnsLayout& E, const Params& 
 
 // Persistent worker: warps claim systems of bucket [begin, end) of the work
 // list until it is empty.  All systems of a bucket have the same K (<= KB).
-template <int KB>
+template <int KB, int KC>
 __global__ void __launch_bounds__(128, min_blocks_for(KB)) ensemble_kernel(EnsLayout E, Params P, const int* __restrict__ order,
                                                        int begin, int end, int K, int* head,
-                                                       long long max_steps) {
-  extern __shared__ double smem[];
-  const Geo g = make_geo(K);
-  const WarpSmem W = warp_smem(smem, K, P.nk);
+                                                       long long max_steps, int steps_total,
+                                                       const long long* epoch, long long budget_ns) {
+  extern __shared__ __align__(16) double smem[];
+  const Geo g = make_geo(KC > 0 ? KC : K);
+  const WarpSmem W = warp_smem(smem, g.K, P.nk);
   const int lane = threadIdx.x & 31;
   const bool leader = g.valid && g.li == 0;
 
@@ -103,9 +104,26 @@ __global__ void __launch_bounds__(128, min_blocks_for(KB)) ensemble_kernel(EnsLa
   S.steps = 0;
   int sys = -1;           // system in this lane's slot (-1: none)
   long long boff = 0;
+  long long step_base = 0;  // steps the system had accumulated before it was loaded (steps_total)
   bool drained = false;   // work list exhausted for this warp (warp-uniform)
+  const long long deadline = budget_ns > 0 ? epoch[0] + budget_ns : 0;
+  bool sliced_out = false;  // time slice over (warp-uniform); independent of drained
 
   while (true) {
+    // ---- time slice over: stop every slot after its current step ----
+    if (deadline != 0 && !sliced_out) {
+      long long now = 0;
+      if (lane == 0) now = global_ns();
+      now = __shfl_sync(FULL, now, 0);
+      if (now >= deadline) {
+        sliced_out = true;
+        drained = true;
+      }
+    }
+    if (sliced_out && S.active) {
+      S.status = ST_MAX_STEPS;
+      S.active = false;
+    }
     // ---- retire finished systems and refill empty slots (warp-uniform) ----
     const bool retire = g.valid && sys >= 0 && !S.active;
     if (__any_sync(FULL, retire)) {
@@ -133,6 +151,11 @@ __global__ void __launch_bounds__(128, min_blocks_for(KB)) ensemble_kernel(EnsLa
       if (fresh) {
         sys = got;
         ens_load<KB>(E, P, g, sys, S, M, W, boff);
+        step_base = (steps_total && E.steps) ? (long long)E.steps[sys] : 0;
+        if (S.active && step_base >= max_steps) {
+          S.status = ST_MAX_STEPS;
+          S.active = false;
+        }
       }
       __syncwarp();
       // first dense sample and initial event value for the fresh systems
@@ -162,57 +185,72 @@ __global__ void __launch_bounds__(128, min_blocks_for(KB)) ensemble_kernel(EnsLa
     const bool stq = step<KB>(g, P, W, M, S);
     if (stq) ens_store_dense<KB>(E, S, g, sys, boff, S.idx);
     after_store(S, P, stq);
-    if (S.active && S.steps >= max_steps) {
+    if (S.active && S.steps + step_base >= max_steps) {
       S.status = ST_MAX_STEPS;
       S.active = false;
     }
   }
 }
 
-template <int KB>
-cudaError_t launch_ensemble(const EnsLayout& E, const Params& P, const int* order, int begin, int end, int K,
-                            int* head, long long max_steps, int blocks, int threads, cudaStream_t stream) {
-  const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, P.nk) * (threads / 32);
-  if (shmem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(ensemble_kernel<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
-    if (e != cudaSuccess) return e;
+size_t max_block_smem(int device) {
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  return (size_t)v;
+}
+
+// Every batched kernel asks for the same (maximum) shared-memory carveout, so
+// that blocks of different bucket kernels can share an SM: with per-kernel
+// carveouts an SM configured for one kernel takes no block of another until it
+// drains, which serialises the buckets.
+template <int KB, int KC>
+cudaError_t configure_ensemble_kernel(size_t shmem) {
+  cudaError_t e = cudaFuncSetAttribute(ensemble_kernel<KB, KC>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared);
+  // the opt-in limit is raised to the device maximum (never lowered again), so
+  // a launch captured earlier with a larger request stays valid
+  if (e == cudaSuccess && shmem > 48 * 1024) {
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    const size_t cap = max_block_smem(dev);
+    if (e == cudaSuccess) {
+      if (shmem > cap) return cudaErrorInvalidValue;
+      e = cudaFuncSetAttribute(ensemble_kernel<KB, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+    }
   }
-  ensemble_kernel<KB><<<blocks, threads, shmem, stream>>>(E, P, order, begin, end, K, head, max_steps);
+  return e;
+}
+
+__global__ void stamp_kernel(long long* epoch) { *epoch = global_ns(); }
+
+cudaError_t launch_stamp(long long* epoch, cudaStream_t stream) {
+  stamp_kernel<<<1, 1, 0, stream>>>(epoch);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ensemble_bucket(const EnsLayout& E, const Params& P, const int* order, int begin, int end,
-                                   int K, int* head, long long max_steps, int blocks, int threads,
-                                   cudaStream_t stream) {
-  switch (kb_for(K)) {
-    case 2: return launch_ensemble<2>(E, P, order, begin, end, K, head, max_steps, blocks, threads, stream);
-    case 4: return launch_ensemble<4>(E, P, order, begin, end, K, head, max_steps, blocks, threads, stream);
-    case 8: return launch_ensemble<8>(E, P, order, begin, end, K, head, max_steps, blocks, threads, stream);
-    case 16: return launch_ensemble<16>(E, P, order, begin, end, K, head, max_steps, blocks, threads, stream);
-    default: return launch_ensemble<32>(E, P, order, begin, end, K, head, max_steps, blocks, threads, stream);
-  }
+                                   int K, int* head, long long max_steps, int steps_total,
+                                   const long long* epoch, long long budget_ns, int blocks, int threads,
+                                   cudaStream_t stream, size_t smem_bytes) {
+  return dispatch_k(K, [&](auto kb, auto kc) {
+    constexpr int KB = decltype(kb)::value, KC = decltype(kc)::value;
+    size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, P.nk) * (threads / 32);
+    if (smem_bytes > shmem) shmem = smem_bytes;
+    cudaError_t e = configure_ensemble_kernel<KB, KC>(shmem);
+    if (e != cudaSuccess) return e;
+    ensemble_kernel<KB, KC><<<blocks, threads, shmem, stream>>>(E, P, order, begin, end, K, head, max_steps,
+                                                                steps_total, epoch, budget_ns);
+    return cudaGetLastError();
+  });
 }
 
 int resident_blocks(int K, int nk, int threads) {
   const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, nk) * (threads / 32);
   int n = 0;
-  cudaError_t e;
-  if (shmem > 48 * 1024) {
-    switch (kb_for(K)) {
-      case 2: cudaFuncSetAttribute(ensemble_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem); break;
-      case 4: cudaFuncSetAttribute(ensemble_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem); break;
-      case 8: cudaFuncSetAttribute(ensemble_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem); break;
-      case 16: cudaFuncSetAttribute(ensemble_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem); break;
-      default: cudaFuncSetAttribute(ensemble_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem); break;
-    }
-  }
-  switch (kb_for(K)) {
-    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<2>, threads, shmem); break;
-    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<4>, threads, shmem); break;
-    case 8: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<8>, threads, shmem); break;
-    case 16: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<16>, threads, shmem); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<32>, threads, shmem); break;
-  }
+  const cudaError_t e = dispatch_k(K, [&](auto kb, auto kc) {
+    constexpr int KB = decltype(kb)::value, KC = decltype(kc)::value;
+    configure_ensemble_kernel<KB, KC>(shmem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<KB, KC>, threads, shmem);
+  });
   return (e == cudaSuccess && n > 0) ? n : 1;
 }
 

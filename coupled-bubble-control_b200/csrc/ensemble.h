@@ -50,9 +50,17 @@ __device__ __forceinline__ long long global_ns() {
   return (long long)t;
 }
 
+// smem_bytes: dynamic shared memory per block; 0 = what the kernel needs.
+// A larger request keeps other blocks off the SM (latency lanes).
+// epoch: device word holding the solve's start time (written by
+// launch_stamp); budget_ns > 0 stops every system budget_ns after it.
 cudaError_t launch_ensemble_bucket(const EnsLayout& E, const Params& P, const int* order, int begin, int end,
-                                   int K, int* head, long long max_steps, int blocks, int threads,
-                                   cudaStream_t stream);
+                                   int K, int* head, long long max_steps, int steps_total,
+                                   const long long* epoch, long long budget_ns, int blocks, int threads,
+                                   cudaStream_t stream, size_t smem_bytes = 0);
+// Writes the device clock (%globaltimer, ns) to *epoch.
+cudaError_t launch_stamp(long long* epoch, cudaStream_t stream);
+size_t max_block_smem(int device);
 int resident_blocks(int K, int nk, int threads);
 
 }  // namespace cbc

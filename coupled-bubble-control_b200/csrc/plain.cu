@@ -43,11 +43,11 @@ __device__ __forceinline__ void ref_store_dense(const RefLayout& L, const LaneSt
   for (int c = 0; c < 4; ++c) L.dense_state[((long long)slot * 4 + c) * NST + s * L.tile + g.li] = S.y[c];
 }
 
-template <int KB>
+template <int KB, int KC>
 __global__ void __launch_bounds__(128, min_blocks_for(KB)) plain_kernel(RefLayout L, Params P, long long budget, int final_launch,
                                                     int* active_counter) {
-  extern __shared__ double smem[];
-  const Geo g = make_geo(L.ups);
+  extern __shared__ __align__(16) double smem[];
+  const Geo g = make_geo(KC > 0 ? KC : L.ups);
   const WarpSmem W = warp_smem(smem, L.ups, P.nk);
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long s = warp * g.G + g.grp;
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(128, min_blocks_for(KB)) plain_kernel(RefLayou
   }
 }
 
-template <int KB>
+template <int KB, int KC>
 cudaError_t launch_plain(const RefLayout& L, const Params& P, long long budget, int final_launch, int* counter,
                          cudaStream_t stream) {
   const int G = 32 / L.ups;
@@ -138,22 +138,19 @@ cudaError_t launch_plain(const RefLayout& L, const Params& P, long long budget, 
   const long long blocks = (warps * 32 + threads - 1) / threads;
   const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(L.ups, P.nk) * (threads / 32);
   if (shmem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(plain_kernel<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+    cudaError_t e =
+        cudaFuncSetAttribute(plain_kernel<KB, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
     if (e != cudaSuccess) return e;
   }
-  plain_kernel<KB><<<(unsigned)blocks, threads, shmem, stream>>>(L, P, budget, final_launch, counter);
+  plain_kernel<KB, KC><<<(unsigned)blocks, threads, shmem, stream>>>(L, P, budget, final_launch, counter);
   return cudaGetLastError();
 }
 
 cudaError_t launch_plain_any(const RefLayout& L, const Params& P, long long budget, int final_launch,
                              int* counter, cudaStream_t stream) {
-  switch (kb_for(L.ups)) {
-    case 2: return launch_plain<2>(L, P, budget, final_launch, counter, stream);
-    case 4: return launch_plain<4>(L, P, budget, final_launch, counter, stream);
-    case 8: return launch_plain<8>(L, P, budget, final_launch, counter, stream);
-    case 16: return launch_plain<16>(L, P, budget, final_launch, counter, stream);
-    default: return launch_plain<32>(L, P, budget, final_launch, counter, stream);
-  }
+  return dispatch_k(L.ups, [&](auto kb, auto kc) {
+    return launch_plain<decltype(kb)::value, decltype(kc)::value>(L, P, budget, final_launch, counter, stream);
+  });
 }
 
 }  // namespace cbc
@@ -179,7 +176,7 @@ int32_t cbc_create(cbc_context** out, int32_t device) {
   cudaSetDevice(device);
   cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
   e = cudaMalloc(&ctx->d_counter, sizeof(int));
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_head, sizeof(int) * CBC_MAX_BUCKETS);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_head, kScheduleBytes);
   if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_counter, sizeof(int));
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
@@ -286,6 +283,7 @@ int32_t cbc_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_buffers* b, 
   if (launch_mode == CBC_LAUNCH_SINGLE) {
     CBC_CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, stream));
     CBC_CUDA_TRY(ctx, launch_plain_any(L, P, launches * (long long)kernel_steps, 1, nullptr, stream));
+    ++ctx->launches;
     CBC_CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, stream));
     n = 1;
     if (stats) {
@@ -301,6 +299,7 @@ int32_t cbc_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_buffers* b, 
       CBC_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int), stream));
       CBC_CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, stream));
       CBC_CUDA_TRY(ctx, launch_plain_any(L, P, kernel_steps, final_launch, ctx->d_counter, stream));
+      ++ctx->launches;
       CBC_CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, stream));
       CBC_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_counter, ctx->d_counter, sizeof(int), cudaMemcpyDeviceToHost, stream));
       CBC_CUDA_TRY(ctx, cudaStreamSynchronize(stream));

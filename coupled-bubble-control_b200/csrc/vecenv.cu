@@ -58,6 +58,7 @@ namespace cbc {
 int32_t enqueue_env_begin(cbc_context* ctx, const cbc_ensemble* e, const cbc_env_io* io, cudaStream_t st) {
   const int threads = 128;
   const int blocks = (e->ns + threads - 1) / threads;
+  ++ctx->launches;
   env_begin_kernel<<<blocks, threads, 0, st>>>(e->ns, io->actions, io->n_act, io->act_stride, io->act_scale,
                                                 const_cast<double*>(e->control_params), e->cp_stride, e->t,
                                                 const_cast<double*>(e->t_end), e->h, e->event, e->status,
@@ -70,6 +71,7 @@ int32_t enqueue_env_end(cbc_context* ctx, const cbc_ensemble* e, const cbc_env_i
   const int threads = 128;
   const long long n = (long long)e->ns * io->K;
   const int blocks = (int)((n + threads - 1) / threads);
+  ++ctx->launches;
   env_end_kernel<<<blocks, threads, 0, st>>>(e->ns, e->nb, (const long long*)e->bubble_offset, e->state,
                                               e->status, io->K, io->obs, io->failed);
   CBC_CUDA_TRY(ctx, cudaGetLastError());

@@ -127,6 +127,10 @@ int32_t cbc_destroy(cbc_context* ctx);
  * next call on the context.  ctx may be NULL (returns the global message). */
 const char* cbc_last_error(const cbc_context* ctx);
 
+/* Kernels this context has enqueued so far (a plan's kernels count once per
+ * cbc_plan_launch).  Diagnostic; no reference counterpart. */
+int64_t cbc_kernel_launches(const cbc_context* ctx);
+
 /* Advances every system of a reference-layout ensemble by at most
  * ceil(max_steps / kernel_steps) * kernel_steps Cash-Karp steps, stopping
  * each system at time_end, at a terminal collision event or on failure.
@@ -204,6 +208,24 @@ typedef struct cbc_work {
   const int32_t* threads;
   const int32_t* blocks_per_sm;
   const float* share;
+  /* Latency lanes (may be NULL).  exclusive[b] > 0 launches bucket b first as
+   * exclusive[b] blocks of 128 threads that each request all shared memory of
+   * an SM, so each runs alone on its SM (minimum per-step latency for the
+   * longest systems); every other bucket then sizes its grids for the
+   * remaining SMs.  share[b] is ignored for such buckets. */
+  const int32_t* exclusive;
+  /* Time slice (0 = none): every system still running budget_ns nanoseconds
+   * (device clock) after the solve started stops after its current step with
+   * status -1, exactly as if max_steps had been reached, and resumes
+   * bit-identically on the next call.  Lets a caller re-plan the order of the
+   * remaining work from the progress observed so far. */
+  int64_t budget_ns;
+  /* 0: max_steps limits the steps of each system within this call (the
+   * reference's kernel_steps).  1: it limits the steps accumulated in
+   * ensemble.steps over all calls, so that a solve split into time slices
+   * stops every system at exactly the step a single call would. */
+  int32_t steps_total;
+  int32_t reserved;
 } cbc_work;
 
 typedef struct cbc_plan cbc_plan;

@@ -139,6 +139,16 @@ double tree_sum(const double* a, int K) {
   return buf[0];
 }
 
+// Pairwise tree without padding: at width w, a[i] += a[i + w] for every i a
+// multiple of 2w with i + w < n, so a lone last element is carried up unchanged:
+// ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + a6).  0.0 for n = 0.
+double tree_sum_open(double* a, int n) {
+  if (n <= 0) return 0.0;
+  for (int w = 1; w < n; w <<= 1)
+    for (int i = 0; i + w < n; i += 2 * w) a[i] = a[i] + a[i + w];
+  return a[0];
+}
+
 // ode_fun + explicit_coupling + implicit_coupling for the whole system
 // (ckm1d_def.py:408-497, :164-248, :250-300, :303-404).
 void rhs(const System& s, const Spec& sp, double t, const double (*y)[4], double (*dy)[4],
@@ -268,12 +278,19 @@ void rhs(const System& s, const Spec& sp, double t, const double (*y)[4], double
   bool conv = false;
   for (int it = 0; it < sp.lin_max_iter; ++it) {
     for (int i = 0; i < K; ++i) {
-      double ar = 0.0, at = 0.0;
+      // partner distance d = 1..K-1 (j = (i + d) mod K) accumulates into
+      // chain (d - 1) mod 4, increasing d within a chain; the chains are
+      // combined by the open pairwise tree: the device kernel's order
+      double cr[4] = {0.0, 0.0, 0.0, 0.0}, ct[4] = {0.0, 0.0, 0.0, 0.0};
       for (int d = 1; d < K; ++d) {
         const int j = (i + d) % K;
-        ar = fma(Am[(size_t)i * K + j], vr[j], fma(Bm[(size_t)i * K + j], vt[j], ar));
-        at = fma(Cm[(size_t)i * K + j], vr[j], fma(Dm[(size_t)i * K + j], vt[j], at));
+        const int c = (d - 1) & 3;
+        cr[c] = fma(Am[(size_t)i * K + j], vr[j], fma(Bm[(size_t)i * K + j], vt[j], cr[c]));
+        ct[c] = fma(Cm[(size_t)i * K + j], vr[j], fma(Dm[(size_t)i * K + j], vt[j], ct[c]));
       }
+      const int nc = K - 1 < 4 ? K - 1 : 4;
+      const double ar = tree_sum_open(cr, nc);
+      const double at = tree_sum_open(ct, nc);
       const double ax0 = fma(ar, cpf0[i], vr[i]);
       const double ax1 = at + vt[i];
       r0[i] = b0[i] - ax0;

@@ -114,3 +114,4 @@ def test_work_list_orders_longest_first():
     assert list(wl.bucket_K) == [8, 3, 2]
     assert list(wl.order) == [3, 1, 4, 2, 5, 0]
     assert list(wl.bucket_begin) == [0, 1, 3, 6]
+

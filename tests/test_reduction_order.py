@@ -53,3 +53,42 @@ def test_tree_differs_from_sequential_for_some_inputs():
     seq = ((a[0] + a[1]) + a[2]) + a[3]
     assert seq == 1.0
     assert oracle_tree(a) == 1.0 + 2e-16 != seq
+
+
+def open_tree(a, N):
+    """The kernels' tree_open over an N-slot register array holding n = len(a)
+    values (unrolled loops over the compile-time N, predicated on n)."""
+    n = len(a)
+    s = list(a) + [0.0] * (N - n)
+    w = 1
+    while w < N:
+        for i in range(0, N - w, 2 * w):
+            if i + w < n:
+                s[i] = s[i] + s[i + w]
+        w <<= 1
+    return s[0] if n > 0 else 0.0
+
+
+def oracle_open(a):
+    """oracle tree_sum_open: at width w < n, a[i] += a[i + w] for i + w < n."""
+    s = list(a)
+    n = len(s)
+    if n == 0:
+        return 0.0
+    w = 1
+    while w < n:
+        for i in range(0, n - w, 2 * w):
+            s[i] = s[i] + s[i + w]
+        w <<= 1
+    return s[0]
+
+
+@pytest.mark.parametrize("KB", [2, 4, 8, 16, 32])
+def test_open_tree_matches_oracle_and_padded_for_norms(KB):
+    rng = np.random.default_rng(KB)
+    for n in range(0, KB + 1):
+        a = (rng.standard_normal(n) * 10.0 ** rng.integers(-8, 8, n)).tolist()
+        assert open_tree(a, KB) == oracle_open(a)
+        nonneg = [x * x for x in a]
+        if n:
+            assert open_tree(nonneg, KB) == oracle_tree(nonneg)
