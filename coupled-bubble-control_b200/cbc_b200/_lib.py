@@ -119,6 +119,8 @@ EXTRA_SIGNATURES: list = [
                               ctypes.POINTER(cbc_work), i64, ctypes.POINTER(P)]),
     ("cbc_env_plan_create", i32, [P, ctypes.POINTER(cbc_spec), ctypes.POINTER(cbc_ensemble),
                                   ctypes.POINTER(cbc_work), i64, ctypes.POINTER(cbc_env_io), ctypes.POINTER(P)]),
+    ("cbc_ensemble_solve_noalloc", i32, [P, ctypes.POINTER(cbc_spec), ctypes.POINTER(cbc_ensemble),
+                                         ctypes.POINTER(cbc_work), i64, P]),
     ("cbc_plan_launch", i32, [P, P]),
     ("cbc_kernel_launches", i64, [P]),
     ("cbc_plan_destroy", i32, [P]),

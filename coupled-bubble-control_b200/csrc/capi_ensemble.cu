@@ -1,5 +1,6 @@
 // capi_ensemble.cu -- C ABI of the batched mixed-K form: direct solve and
 // CUDA-graph plans.  See ensemble.cu for the device side.
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -106,18 +107,37 @@ constexpr float kStartFill = 0.85f;
 
 constexpr int kExclusiveThreads = 128;
 
-struct Grids {
-  std::vector<int> first, second, threads;
-  std::vector<size_t> smem;      // dynamic shared memory request (0: what the kernel needs)
-  std::vector<char> exclusive;
+// Per-bucket launch parameters.  The storage is a template parameter so that
+// the allocation-free entry point can use fixed arrays (FixedVec) while the
+// others keep std::vector.
+template <class T>
+using HeapVec = std::vector<T>;
+
+template <class T>
+struct FixedVec {
+  T v[CBC_MAX_BUCKETS];
+  void assign(size_t n, T x) {
+    for (size_t i = 0; i < n && i < CBC_MAX_BUCKETS; ++i) v[i] = x;
+  }
+  T& operator[](size_t i) { return v[i]; }
+  const T& operator[](size_t i) const { return v[i]; }
 };
+
+template <template <class> class V>
+struct GridsT {
+  V<int> first, second, threads;
+  V<size_t> smem;      // dynamic shared memory request (0: what the kernel needs)
+  V<char> exclusive;
+};
+using Grids = GridsT<HeapVec>;
 
 static bool is_exclusive(const cbc_work* w, int b) {
   return w->exclusive && w->exclusive[b] > 0 && w->bucket_begin[b + 1] > w->bucket_begin[b];
 }
 
-static Grids grid_sizes(cbc_context* ctx, const cbc_spec* spec, const cbc_work* w) {
-  Grids g;
+template <class G = Grids>
+static G grid_sizes(cbc_context* ctx, const cbc_spec* spec, const cbc_work* w) {
+  G g;
   g.first.assign(w->nbuckets, 0);
   g.second.assign(w->nbuckets, 0);
   g.threads.assign(w->nbuckets, kDefaultThreads);
@@ -172,8 +192,9 @@ static Grids grid_sizes(cbc_context* ctx, const cbc_spec* spec, const cbc_work* 
 
 // Enqueues the whole batched solve on `stream`: every bucket on its own
 // forked stream (ctx->side[b]), joined back into `stream`.
+template <class G>
 static int32_t enqueue(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e, const cbc_work* w,
-                       const Grids& grids, int64_t max_steps, int* d_head, cudaStream_t stream) {
+                       const G& grids, int64_t max_steps, int* d_head, cudaStream_t stream) {
   const EnsLayout E = make_layout(e);
   const Params P = make_params(*spec);
   CBC_CUDA_TRY(ctx, cudaMemsetAsync(d_head, 0, sizeof(int) * w->nbuckets, stream));
@@ -229,6 +250,48 @@ int32_t cbc_ensemble_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_ens
   DeviceGuard dg(ctx->device);
   const Grids grids = grid_sizes(ctx, spec, w);
   return enqueue(ctx, spec, e, w, grids, max_steps, ctx->d_head, (cudaStream_t)stream);
+}
+
+// ---- allocation-free batched solve -------------------------------------
+// Scheduling scratch of cbc_ensemble_solve_noalloc: CBC_MAX_BUCKETS work-list
+// cursors, then the epoch word (kScheduleBytes = 144 bytes per device).  The
+// cursors are zeroed by every call on its stream before its kernels run; the
+// epoch word is written by the call's stamp kernel when budget_ns > 0.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScheduleBytes];
+static_assert(kScheduleBytes == sizeof(int) * CBC_MAX_BUCKETS + 2 * sizeof(long long), "scratch layout");
+
+constexpr int kNoallocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+int32_t cbc_ensemble_solve_noalloc(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e,
+                                   const cbc_work* w, int64_t max_steps, void* stream) {
+  if (!ctx) return fail(nullptr, CBC_E_INVALID, "context is NULL");
+  ctx->err.clear();
+  int32_t rc = check_ensemble(ctx, spec, e, w);
+  if (rc) return rc;
+  if (max_steps < 1) return fail(ctx, CBC_E_INVALID, "max_steps must be >= 1");
+  if (w->nbuckets > CBC_MAX_BUCKETS)
+    return fail(ctx, CBC_E_UNSUPPORTED, "cbc_ensemble_solve_noalloc: %d buckets exceed its static scratch of %d",
+                w->nbuckets, CBC_MAX_BUCKETS);
+  if (ctx->device < 0 || ctx->device >= kNoallocMaxDevices)
+    return fail(ctx, CBC_E_UNSUPPORTED, "cbc_ensemble_solve_noalloc: device %d beyond %d", ctx->device,
+                kNoallocMaxDevices);
+  DeviceGuard dg(ctx->device);
+  void* scratch = nullptr;
+  {
+    // set-up once per device, with the device current
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[ctx->device]) {
+      void* p = nullptr;
+      const cudaError_t ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (ce != cudaSuccess || !p) return fail(ctx, CBC_E_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(ce));
+      g_noalloc_ptr[ctx->device] = p;
+    }
+    scratch = g_noalloc_ptr[ctx->device];
+  }
+  const auto grids = grid_sizes<GridsT<FixedVec>>(ctx, spec, w);
+  return enqueue(ctx, spec, e, w, grids, max_steps, static_cast<int*>(scratch), (cudaStream_t)stream);
 }
 
 int32_t cbc_plan_create(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e, const cbc_work* w,

@@ -239,6 +239,20 @@ typedef struct cbc_plan cbc_plan;
 int32_t cbc_ensemble_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* ens,
                            const cbc_work* work, int64_t max_steps, void* stream);
 
+/* The same batched solve, allocating nothing: no cudaMalloc / cudaFree and no
+ * host heap on success.  Its scheduling scratch (the work-list cursors and
+ * the time-slice epoch, 144 bytes) is a static device array of the library,
+ * whose address is looked up once per device (cudaGetSymbolAddress) on the
+ * first call with that context's device; make that first call outside any
+ * stream capture.  The cursors are zeroed by each call on `stream` before its
+ * kernels.  Work lists of more than CBC_MAX_BUCKETS buckets are rejected
+ * (CBC_E_INVALID from the common checks).  The scratch is shared by all calls
+ * on a device: calls whose executions overlap in time (different streams,
+ * no ordering between them) race on it and must not be issued.  No
+ * counterpart in the reference. */
+int32_t cbc_ensemble_solve_noalloc(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* ens,
+                                   const cbc_work* work, int64_t max_steps, void* stream);
+
 /* Captures the same launch sequence into a CUDA graph bound to these buffers;
  * cbc_plan_launch replays it on `stream` (one graph launch per solve). */
 int32_t cbc_plan_create(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* ens,
