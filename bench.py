@@ -196,14 +196,14 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def make_plan(ens, schedule: str):
+def make_plan(ens, schedule: str, max_steps: int = MAX_STEPS):
     """adaptive: time slices with re-planning and latency lanes; pilot: one
     measured re-ordering after a short pilot pass; span: longest span first."""
     if schedule == "adaptive":
-        return ens.adaptive_plan(MAX_STEPS)
+        return ens.adaptive_plan(max_steps)
     if schedule == "pilot":
-        return ens.scheduled_plan(MAX_STEPS, pilot_steps=256)
-    return ens.plan(MAX_STEPS)
+        return ens.scheduled_plan(max_steps, pilot_steps=min(256, max_steps - 1))
+    return ens.plan(max_steps)
 
 
 def batched_once(scene, dev_index: int, schedule: str) -> float:
@@ -288,7 +288,7 @@ def run_b200(args):
     scene = scenes.mixed_k(ns=args.ns, seed=rank_seed(rank))
     ens = Ensemble.from_scene(scene, device=local)
     ens.to_device()
-    plan = make_plan(ens, args.schedule)
+    plan = make_plan(ens, args.schedule, args.max_steps)
     nbuckets = int(np.unique(scene.K).size)
     # pristine device copy of the initial state for the per-step reset
     pristine = {k: v.clone() for k, v in ens.dev.items()}
@@ -383,7 +383,7 @@ def run_b200(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"mixed_k_{args.ns}", "ns_per_gpu": args.ns, "K": [2, 3, 4, 6, 8],
                        "K_weights": [0.4, 0.2, 0.2, 0.1, 0.1], "span_periods": [5, 50], "rtol": 1e-9,
-                       "atol": 1e-9, "max_steps": MAX_STEPS, "field": "SW_A 25+50 kHz",
+                       "atol": 1e-9, "max_steps": args.max_steps, "field": "SW_A 25+50 kHz",
                        "l2": "256 MiB buffer written before every step", "parallelism": f"replicas{world}",
                        "schedule": args.schedule},
             "work": {"advanced_system_periods_per_step": adv, "nominal_system_periods": float(np.sum(scene.t_end)),
@@ -426,6 +426,8 @@ def main():
     ap.add_argument("--no-env", dest="env", action="store_false")
     ap.add_argument("--plain-ns", type=int, default=16384, help="systems used for the batched-vs-plain ratio")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--max-steps", type=int, default=MAX_STEPS,
+                    help="step cap per system (the reference's max_steps); small values make short profiling cases")
     ap.add_argument("--schedule", default="adaptive", choices=["adaptive", "pilot", "span"],
                     help="pilot: measured longest-first re-ordering after a pilot pass; span: longest span first")
     args = ap.parse_args()
