@@ -37,6 +37,23 @@
 #define CBC_HD static inline
 #endif
 
+// Coefficient tables.  On the device they live in constant memory, so FP64
+// fma instructions take them as constant-bank operands instead of
+// rematerialising every 64-bit immediate in registers; the host (and the CPU
+// oracle) reads the identical constexpr values.
+#if defined(__CUDACC__)
+#define CBCM_TABLE(name, ...)                                  \
+  static constexpr double name##_h[] = {__VA_ARGS__};          \
+  static __constant__ const double name##_d[] = {__VA_ARGS__};
+#else
+#define CBCM_TABLE(name, ...) static constexpr double name##_h[] = {__VA_ARGS__};
+#endif
+#if defined(__CUDA_ARCH__)
+#define CBCM_K(name, i) (name##_d[i])
+#else
+#define CBCM_K(name, i) (name##_h[i])
+#endif
+
 namespace cbcm {
 
 CBC_HD double bits_to_double(uint64_t u) {
@@ -94,6 +111,10 @@ static constexpr double C14 = -0x1.93974a8c07c9dp-37;
 static constexpr double C16 = 0x1.ae7f3e733b81fp-45;
 static constexpr double C18 = -0x1.6827863b97d97p-53;
 
+CBCM_TABLE(SC_RED, PIO2_1, PIO2_2, PIO2_3, TWO_OVER_PI)
+CBCM_TABLE(SIN_P, S3, S5, S7, S9, S11, S13, S15, S17, S19)
+CBCM_TABLE(COS_P, C2, C4, C6, C8, C10, C12, C14, C16, C18)
+
 // sin and cos of x together.  NaN/inf input gives NaN outputs.
 CBC_HD void sincos(double x, double* s, double* c) {
   if (!isfinite_(x)) {
@@ -101,28 +122,19 @@ CBC_HD void sincos(double x, double* s, double* c) {
     *c = *s;
     return;
   }
-  double kd = rint_(x * TWO_OVER_PI);
-  double r = fma_(-kd, PIO2_1, x);
-  r = fma_(-kd, PIO2_2, r);
-  r = fma_(-kd, PIO2_3, r);
+  double kd = rint_(x * CBCM_K(SC_RED, 3));
+  double r = fma_(-kd, CBCM_K(SC_RED, 0), x);
+  r = fma_(-kd, CBCM_K(SC_RED, 1), r);
+  r = fma_(-kd, CBCM_K(SC_RED, 2), r);
   double z = r * r;
-  double ps = fma_(S19, z, S17);
-  ps = fma_(ps, z, S15);
-  ps = fma_(ps, z, S13);
-  ps = fma_(ps, z, S11);
-  ps = fma_(ps, z, S9);
-  ps = fma_(ps, z, S7);
-  ps = fma_(ps, z, S5);
-  ps = fma_(ps, z, S3);
+  // Horner from the highest coefficient down (S19 ... S3, C18 ... C2)
+  double ps = fma_(CBCM_K(SIN_P, 8), z, CBCM_K(SIN_P, 7));
+#pragma unroll
+  for (int i = 6; i >= 0; --i) ps = fma_(ps, z, CBCM_K(SIN_P, i));
   double sr = fma_(r * z, ps, r);
-  double pc = fma_(C18, z, C16);
-  pc = fma_(pc, z, C14);
-  pc = fma_(pc, z, C12);
-  pc = fma_(pc, z, C10);
-  pc = fma_(pc, z, C8);
-  pc = fma_(pc, z, C6);
-  pc = fma_(pc, z, C4);
-  pc = fma_(pc, z, C2);
+  double pc = fma_(CBCM_K(COS_P, 8), z, CBCM_K(COS_P, 7));
+#pragma unroll
+  for (int i = 6; i >= 0; --i) pc = fma_(pc, z, CBCM_K(COS_P, i));
   double cr = fma_(z, pc, 1.0);
   // quadrant q = k mod 4 from the low two bits of k (two's complement keeps
   // k mod 4 in the low bits for negative k).
@@ -151,26 +163,22 @@ static constexpr double E11 = 0x1.ae64567f544e4p-26;
 static constexpr double E12 = 0x1.1eed8eff8d898p-29;
 static constexpr double E13 = 0x1.6124613a86d09p-33;
 
+CBCM_TABLE(EXP_RED, LOG2E, LN2_HI, LN2_LO)
+CBCM_TABLE(EXP_P, E2, E3, E4, E5, E6, E7, E8, E9, E10, E11, E12, E13)
+
 // 2^n for integer n in [-1022, 1023] (exact)
 CBC_HD double pow2i(int n) { return bits_to_double((uint64_t)(n + 1023) << 52); }
 
 CBC_HD double exp(double x) {
   if (!(x < 709.8)) return (x != x) ? x : bits_to_double(0x7ff0000000000000ULL);
   if (x < -745.2) return 0.0;
-  double nd = rint_(x * LOG2E);
-  double r = fma_(-nd, LN2_HI, x);
-  r = fma_(-nd, LN2_LO, r);
-  double p = fma_(E13, r, E12);
-  p = fma_(p, r, E11);
-  p = fma_(p, r, E10);
-  p = fma_(p, r, E9);
-  p = fma_(p, r, E8);
-  p = fma_(p, r, E7);
-  p = fma_(p, r, E6);
-  p = fma_(p, r, E5);
-  p = fma_(p, r, E4);
-  p = fma_(p, r, E3);
-  p = fma_(p, r, E2);
+  double nd = rint_(x * CBCM_K(EXP_RED, 0));
+  double r = fma_(-nd, CBCM_K(EXP_RED, 1), x);
+  r = fma_(-nd, CBCM_K(EXP_RED, 2), r);
+  // Horner E13 ... E2, then 1, 1
+  double p = fma_(CBCM_K(EXP_P, 11), r, CBCM_K(EXP_P, 10));
+#pragma unroll
+  for (int i = 9; i >= 0; --i) p = fma_(p, r, CBCM_K(EXP_P, i));
   p = fma_(p, r, 1.0);
   p = fma_(p, r, 1.0);
   int n = (int)nd;
@@ -192,6 +200,9 @@ static constexpr double L17 = 0x1.e1e1e1e1e1e1ep-5;
 static constexpr double L19 = 0x1.af286bca1af28p-5;
 static constexpr double L21 = 0x1.8618618618618p-5;
 static constexpr double L23 = 0x1.642c8590b2164p-5;
+
+CBCM_TABLE(LOG_P, L3, L5, L7, L9, L11, L13, L15, L17, L19, L21, L23)
+CBCM_TABLE(LOG_C, LN2_HI, LN2_LO)
 
 CBC_HD double log(double x) {
   if (!(x > 0.0)) {
@@ -215,20 +226,14 @@ CBC_HD double log(double x) {
   e += eadj;
   double f = (m - 1.0) / (m + 1.0);
   double s = f * f;
-  double p = fma_(L23, s, L21);
-  p = fma_(p, s, L19);
-  p = fma_(p, s, L17);
-  p = fma_(p, s, L15);
-  p = fma_(p, s, L13);
-  p = fma_(p, s, L11);
-  p = fma_(p, s, L9);
-  p = fma_(p, s, L7);
-  p = fma_(p, s, L5);
-  p = fma_(p, s, L3);
+  // Horner L23 ... L3
+  double p = fma_(CBCM_K(LOG_P, 10), s, CBCM_K(LOG_P, 9));
+#pragma unroll
+  for (int i = 8; i >= 0; --i) p = fma_(p, s, CBCM_K(LOG_P, i));
   double f2 = f + f;
   double logm = fma_(f2 * s, p, f2);
   double ed = (double)e;
-  return fma_(ed, LN2_HI, fma_(ed, LN2_LO, logm));
+  return fma_(ed, CBCM_K(LOG_C, 0), fma_(ed, CBCM_K(LOG_C, 1), logm));
 }
 
 // x^y for x > 0 (x <= 0 gives NaN, matching the physical meaning of a

@@ -147,6 +147,7 @@ struct WarpSmem {
   double* up;   // [15][32]    bubble constants, lane-private columns
   double* ks;   // [6][4][32]  stage derivatives, lane-private columns
   double* xv;   // [2][32] double2 partner-state exchange records
+  double* cm;   // [3][K-1][32] coupling coefficients of each lane's partners d = 1..K-1
 };
 
 constexpr int XV_DOUBLES = 4 * 32;
@@ -156,7 +157,7 @@ constexpr int XV_DOUBLES = 4 * 32;
 __host__ __device__ inline int hc_doubles(int K, int nk) { return (HC_PER_K * nk * (32 / K) + 1) & ~1; }
 
 __host__ __device__ inline int smem_doubles_per_warp(int K, int nk) {
-  return hc_doubles(K, nk) + NUPS * 32 + 24 * 32 + XV_DOUBLES;
+  return hc_doubles(K, nk) + NUPS * 32 + 24 * 32 + XV_DOUBLES + 3 * (K - 1) * 32;
 }
 
 __device__ __forceinline__ WarpSmem warp_smem(double* base, int K, int nk) {
@@ -166,6 +167,7 @@ __device__ __forceinline__ WarpSmem warp_smem(double* base, int K, int nk) {
   w.up = p + hc_doubles(K, nk);
   w.ks = w.up + NUPS * 32;
   w.xv = w.ks + 24 * 32;
+  w.cm = w.xv + XV_DOUBLES;
   return w;
 }
 
@@ -174,6 +176,21 @@ struct MView {
   const double* __restrict__ m;  // points at M(0, 0, i)
   long long sc, sj;
 };
+
+// Copies this lane's coupling coefficients M(c, j, i) for its partners
+// j = (i + d) mod K, d = 1..K-1, into shared memory: they are constant for the
+// whole solve and are read every RHS evaluation.
+__device__ __forceinline__ void store_coupling(const WarpSmem& w, const Geo& g, const MView& M) {
+  for (int d = 1; d < g.K; ++d) {
+    const int j = partner_lane(g, d) - g.base;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) w.cm[(c * (g.K - 1) + d - 1) * 32 + g.lane] = M.m[c * M.sc + j * M.sj];
+  }
+}
+
+__device__ __forceinline__ double cmv(const WarpSmem& w, const Geo& g, int c, int d) {
+  return w.cm[(c * (g.K - 1) + d - 1) * 32 + g.lane];
+}
 
 // Per-lane integrator state (bubble + copies of the system scalars).
 struct LaneState {
@@ -434,9 +451,9 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
         const double rd2 = rd * rd;
         const double srd2 = rd2 * sg;
         const double rd3 = rd2 * rd;
-        const double m0 = __ldg(M.m + j * M.sj);
-        const double m1 = __ldg(M.m + M.sc + j * M.sj);
-        const double m2 = __ldg(M.m + 2 * M.sc + j * M.sj);
+        const double m0 = cmv(W, g, 0, d);
+        const double m1 = cmv(W, g, 1, d);
+        const double m2 = cmv(W, g, 2, d);
         double t0 = fma(2.5 * srd2, h2j, rd3 * h4j);
         t0 = fma(2.0 * rd, h0j, t0);
         g0 = fma(-m0, t0, g0);
@@ -531,6 +548,19 @@ __device__ __forceinline__ void prologue(LaneState& S, const Params& P, double g
   S.lin_iters = 0;
 }
 
+// State at Cash-Karp stage ST: y + h * sum_{m < ST} b[ST][m] k_m, the sum
+// accumulated in increasing m (coefficients and loop fully compile-time).
+template <int ST>
+__device__ __forceinline__ void stage_state(const double* ks, double h, const double y[4], double ys[4]) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    double acc = kStageB[ST][0] * ks[c * 32];
+#pragma unroll
+    for (int m = 1; m < ST; ++m) acc = fma(kStageB[ST][m], ks[(m * 4 + c) * 32], acc);
+    ys[c] = fma(h, acc, y[c]);
+  }
+}
+
 // One adaptive Cash-Karp step for every active group of the warp
 // (stepper.py:362-677).  Returns true (per lane) if a dense sample must be
 // stored after this step; the caller writes it.
@@ -561,16 +591,16 @@ __device__ __forceinline__ bool step(const Geo& g, const Params& P, const WarpSm
 #pragma unroll 1
   for (int st = 0; st < 6; ++st) {
     double ys[4];
-    if (st == 0) {
+    switch (st) {
+      case 0:
 #pragma unroll
-      for (int c = 0; c < 4; ++c) ys[c] = S.y[c];
-    } else {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        double acc = kStageB[st][0] * ks[c * 32];
-        for (int m = 1; m < st; ++m) acc = fma(kStageB[st][m], ks[(m * 4 + c) * 32], acc);
-        ys[c] = fma(h, acc, S.y[c]);
-      }
+        for (int c = 0; c < 4; ++c) ys[c] = S.y[c];
+        break;
+      case 1: stage_state<1>(ks, h, S.y, ys); break;
+      case 2: stage_state<2>(ks, h, S.y, ys); break;
+      case 3: stage_state<3>(ks, h, S.y, ys); break;
+      case 4: stage_state<4>(ks, h, S.y, ys); break;
+      default: stage_state<5>(ks, h, S.y, ys); break;
     }
     const double ts = (st == 0) ? t : fma(kStageA[st], h, t);
     double kk[4];

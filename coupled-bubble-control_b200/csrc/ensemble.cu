@@ -58,6 +58,7 @@ __device__ __forceinline__ void ens_load(const EnsLayout& E, const Params& P, co
   M.m = E.coupling + E.coupling_offset[s] + g.li;
   M.sc = (long long)g.K * g.K;
   M.sj = g.K;
+  store_coupling(W, g, M);
   if (g.li == 0) store_harmonics(W, g, sp[1], sp[2], sp[4], E.control_params + (long long)s * E.cp_stride, P.nk, 1);
 }
 

@@ -67,6 +67,7 @@ __global__ void __launch_bounds__(128, min_blocks_for(KB)) plain_kernel(RefLayou
 #pragma unroll
     for (int c = 0; c < 4; ++c) S.y[c] = L.actual_state[c * NST + lane_off];
     store_bubble_consts(W, g, L.unit_params + lane_off, NST);
+    store_coupling(W, g, M);
     S.sp0 = L.system_params[0 * (long long)L.ns + s];
     S.sp3 = L.system_params[3 * (long long)L.ns + s];
     S.t = L.actual_time[s];
