@@ -395,27 +395,6 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
       }
     }
   }
-  const double u7 = upv(W, g, 7);
-  const double q = fma(u7, x2, 1.0);
-  double N = fma(upv(W, g, 1), x2, upv(W, g, 0)) * p;
-  N = fma(-upv(W, g, 2), q, N);
-  N = fma(-upv(W, g, 3), rx0, N);
-  N = fma(-(upv(W, g, 4) * x2), rx0, N);
-  const double w = fma(-upv(W, g, 13), x2, 1.0);
-  N = fma((-1.5 * w) * x2, x2, N);
-  N = fma(-(q * upv(W, g, 5)), pa, N);
-  N = fma(-(upv(W, g, 6) * pt), x0, N);
-  N = fma(upv(W, g, 8) * x3, x3, N);
-  const double D = fma(-(u7 * x0), x2, x0) + upv(W, g, 14);
-  const double rD = 1.0 / D;
-  const double x02 = x0 * x0;
-  const double x03 = x02 * x0;
-  const double Fb1 = -(upv(W, g, 10) * x03) * px;
-  const double Fd = -(upv(W, g, 11) * x0) * fma(x3, sp3, -ux);
-  const double rx03 = (rx0 * rx0) * rx0;
-  double b0 = N * rD;
-  double b1 = fma((3.0 * (Fb1 + Fd)) * upv(W, g, 9), rx03, -(((3.0 * x2) * rx0) * x3));
-  const double cpf0 = rD, cpf1 = x3 * rD, cpf2 = x2 * rx0, cpf3 = rx0 * rx0;
 
   // ---- explicit coupling + matrix of the implicit system over partners ----
   double g0 = 0.0, g1 = 0.0, tn = 0.0, tg2 = 0.0, tg3 = 0.0;
@@ -435,8 +414,9 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
       // owning lane computes them (cheaper than exchanging seven terms)
       const double2 xa = xv2[src], xb = xv2[32 + src];
       const double xj0 = xa.x, xj1 = xa.y, xj2 = xb.x, xj3 = xb.y;
-      if (on) {
-        const int j = src - g.base;
+      // evaluated for every lane (no branch): lanes of finished systems
+      // compute terms that are never used
+      {
         const double j02 = xj0 * xj0;
         const double j03 = j02 * xj0;
         const double h0j = xj0 * (xj2 * xj2);
@@ -470,6 +450,30 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
       }
     }
   }
+  // Keller--Miksis numerator / denominator of this bubble (after the partner
+  // loop in program order, so that the division and log/exp chain feeding p
+  // overlaps with the partner terms)
+  const double u7 = upv(W, g, 7);
+  const double q = fma(u7, x2, 1.0);
+  double N = fma(upv(W, g, 1), x2, upv(W, g, 0)) * p;
+  N = fma(-upv(W, g, 2), q, N);
+  N = fma(-upv(W, g, 3), rx0, N);
+  N = fma(-(upv(W, g, 4) * x2), rx0, N);
+  const double w = fma(-upv(W, g, 13), x2, 1.0);
+  N = fma((-1.5 * w) * x2, x2, N);
+  N = fma(-(q * upv(W, g, 5)), pa, N);
+  N = fma(-(upv(W, g, 6) * pt), x0, N);
+  N = fma(upv(W, g, 8) * x3, x3, N);
+  const double D = fma(-(u7 * x0), x2, x0) + upv(W, g, 14);
+  const double rD = 1.0 / D;
+  const double x02 = x0 * x0;
+  const double x03 = x02 * x0;
+  const double Fb1 = -(upv(W, g, 10) * x03) * px;
+  const double Fd = -(upv(W, g, 11) * x0) * fma(x3, sp3, -ux);
+  const double rx03 = (rx0 * rx0) * rx0;
+  double b0 = N * rD;
+  double b1 = fma((3.0 * (Fb1 + Fd)) * upv(W, g, 9), rx03, -(((3.0 * x2) * rx0) * x3));
+  const double cpf0 = rD, cpf1 = x3 * rD, cpf2 = x2 * rx0, cpf3 = rx0 * rx0;
   b0 = fma(g0, cpf0, fma(g1, cpf1, b0));
   b1 = b1 + fma(tg2, cpf2, fma(tg3, cpf3, tn));
 
