@@ -116,12 +116,11 @@ CBCM_TABLE(SIN_P, S3, S5, S7, S9, S11, S13, S15, S17, S19)
 CBCM_TABLE(COS_P, C2, C4, C6, C8, C10, C12, C14, C16, C18)
 
 // sin and cos of x together.  NaN/inf input gives NaN outputs.
-CBC_HD void sincos(double x, double* s, double* c) {
-  if (!isfinite_(x)) {
-    *s = x - x;  // NaN for +-inf and NaN
-    *c = *s;
-    return;
-  }
+// Branch-free: the main path runs on a sanitised argument and the special
+// case is selected at the end (lets the compiler interleave independent calls).
+CBC_HD void sincos(double x_in, double* s, double* c) {
+  const bool fin = isfinite_(x_in);
+  const double x = fin ? x_in : 0.0;
   double kd = rint_(x * CBCM_K(SC_RED, 3));
   double r = fma_(-kd, CBCM_K(SC_RED, 0), x);
   r = fma_(-kd, CBCM_K(SC_RED, 1), r);
@@ -143,8 +142,9 @@ CBC_HD void sincos(double x, double* s, double* c) {
   int q = (int)(ki & 3);
   double a = (q & 1) ? cr : sr;
   double b = (q & 1) ? sr : cr;
-  *s = (q & 2) ? -a : a;
-  *c = ((q + 1) & 2) ? -b : b;
+  const double nan_ = x_in - x_in;  // NaN for +-inf and NaN
+  *s = fin ? ((q & 2) ? -a : a) : nan_;
+  *c = fin ? (((q + 1) & 2) ? -b : b) : nan_;
 }
 
 static constexpr double LOG2E = 0x1.71547652b82fep+0;
@@ -169,9 +169,13 @@ CBCM_TABLE(EXP_P, E2, E3, E4, E5, E6, E7, E8, E9, E10, E11, E12, E13)
 // 2^n for integer n in [-1022, 1023] (exact)
 CBC_HD double pow2i(int n) { return bits_to_double((uint64_t)(n + 1023) << 52); }
 
-CBC_HD double exp(double x) {
-  if (!(x < 709.8)) return (x != x) ? x : bits_to_double(0x7ff0000000000000ULL);
-  if (x < -745.2) return 0.0;
+// Branch-free (special cases selected at the end); the scaling by 2^n is
+// split in two factors so that results in the subnormal range round once
+// (the second factor is exactly 1 when |n| <= 1000).
+CBC_HD double exp(double x_in) {
+  const bool big = !(x_in < 709.8);  // also NaN and +inf
+  const bool tiny = x_in < -745.2;
+  const double x = (big || tiny) ? 0.0 : x_in;
   double nd = rint_(x * CBCM_K(EXP_RED, 0));
   double r = fma_(-nd, CBCM_K(EXP_RED, 1), x);
   r = fma_(-nd, CBCM_K(EXP_RED, 2), r);
@@ -181,11 +185,11 @@ CBC_HD double exp(double x) {
   for (int i = 9; i >= 0; --i) p = fma_(p, r, CBCM_K(EXP_P, i));
   p = fma_(p, r, 1.0);
   p = fma_(p, r, 1.0);
-  int n = (int)nd;
-  // split the scaling so that results in the subnormal range round once
-  if (n > 1000) return p * pow2i(1000) * pow2i(n - 1000);
-  if (n < -1000) return p * pow2i(-1000) * pow2i(n + 1000);
-  return p * pow2i(n);
+  const int n = (int)nd;
+  const int n1 = n > 1000 ? 1000 : (n < -1000 ? -1000 : n);
+  const double res = (p * pow2i(n1)) * pow2i(n - n1);
+  const double ovf = (x_in != x_in) ? x_in : bits_to_double(0x7ff0000000000000ULL);
+  return big ? ovf : (tiny ? 0.0 : res);
 }
 
 static constexpr double SQRT1_2 = 0x1.6a09e667f3bcdp-1;
@@ -204,25 +208,21 @@ static constexpr double L23 = 0x1.642c8590b2164p-5;
 CBCM_TABLE(LOG_P, L3, L5, L7, L9, L11, L13, L15, L17, L19, L21, L23)
 CBCM_TABLE(LOG_C, LN2_HI, LN2_LO)
 
-CBC_HD double log(double x) {
-  if (!(x > 0.0)) {
-    if (x == 0.0) return -bits_to_double(0x7ff0000000000000ULL);
-    return bits_to_double(0x7ff8000000000000ULL);  // x < 0 or NaN
-  }
-  if (!isfinite_(x)) return x;  // +inf
-  int eadj = 0;
-  if (x < 0x1p-1022) {  // subnormal: scale into the normal range (exact)
-    x = x * 0x1p54;
-    eadj = -54;
-  }
+// Branch-free (special cases selected at the end).
+CBC_HD double log(double x_in) {
+  const bool pos = x_in > 0.0;  // false for +-0, negatives and NaN
+  const bool main_path = pos && isfinite_(x_in);
+  double x = main_path ? x_in : 1.0;
+  const bool sub = x < 0x1p-1022;  // subnormal: scale into the normal range (exact)
+  x = sub ? x * 0x1p54 : x;
+  const int eadj = sub ? -54 : 0;
   uint64_t u = double_to_bits(x);
   int e = (int)((u >> 52) & 0x7ff) - 1023;
   // m in [1, 2)
   double m = bits_to_double((u & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL);
-  if (m > 2.0 * SQRT1_2) {
-    m = m * 0.5;
-    e += 1;
-  }
+  const bool hi = m > 2.0 * SQRT1_2;
+  m = hi ? m * 0.5 : m;
+  e += hi ? 1 : 0;
   e += eadj;
   double f = (m - 1.0) / (m + 1.0);
   double s = f * f;
@@ -233,7 +233,11 @@ CBC_HD double log(double x) {
   double f2 = f + f;
   double logm = fma_(f2 * s, p, f2);
   double ed = (double)e;
-  return fma_(ed, CBCM_K(LOG_C, 0), fma_(ed, CBCM_K(LOG_C, 1), logm));
+  const double res = fma_(ed, CBCM_K(LOG_C, 0), fma_(ed, CBCM_K(LOG_C, 1), logm));
+  // x == 0: -inf; x < 0 or NaN: NaN; +inf: +inf
+  const double special = (x_in == 0.0) ? -bits_to_double(0x7ff0000000000000ULL)
+                                       : (pos ? x_in : bits_to_double(0x7ff8000000000000ULL));
+  return main_path ? res : special;
 }
 
 // x^y for x > 0 (x <= 0 gives NaN, matching the physical meaning of a

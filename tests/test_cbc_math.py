@@ -41,3 +41,22 @@ def test_exp_log_pow():
     assert np.isnan(oracle.math_eval(3, np.array([-1.0]))[0])
     assert oracle.math_eval(2, np.array([800.0]))[0] == np.inf
     assert oracle.math_eval(2, np.array([-800.0]))[0] == 0.0
+
+
+def test_special_values():
+    """Non-finite, zero, subnormal and range-edge arguments (the routines
+    select these results instead of branching)."""
+    inf, nan = np.inf, np.nan
+    e = oracle.math_eval(2, np.array([nan, inf, -inf, 709.7, -745.1, -740.0, -1e-320, 0.0, -0.0]))
+    assert np.isnan(e[0]) and e[1] == inf and e[2] == 0.0
+    ref = np.exp(np.array([709.7, -745.1, -740.0]))
+    assert np.all(_ulps(e[3:6], ref) <= 2.0)
+    assert e[6] == 1.0 and e[7] == 1.0 and e[8] == 1.0
+    lg = oracle.math_eval(3, np.array([nan, inf, -inf, -0.0, 0.0, 5e-324, 2.2e-308, 1.7e308, -2.0]))
+    assert np.isnan(lg[0]) and lg[1] == inf and np.isnan(lg[2]) and lg[3] == -inf and lg[4] == -inf
+    assert np.all(_ulps(lg[5:8], np.log(np.array([5e-324, 2.2e-308, 1.7e308]))) <= 2.0)
+    assert np.isnan(lg[8])
+    for kind in (0, 1):
+        v = oracle.math_eval(kind, np.array([inf, -inf, nan, 0.0, -0.0]))
+        assert np.all(np.isnan(v[:3]))
+    assert oracle.math_eval(0, np.array([0.0]))[0] == 0.0 and oracle.math_eval(1, np.array([0.0]))[0] == 1.0
