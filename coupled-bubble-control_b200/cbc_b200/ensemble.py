@@ -39,10 +39,10 @@ class WorkList:
 
 # Steady-state cost of one step attempt on a full B200 (ns), measured on
 # uniform-K ensembles with every slot busy (no tail); other K are interpolated.
-STEP_NS = {1: 0.55, 2: 0.80, 3: 2.09, 4: 2.57, 6: 7.50, 8: 10.35}
+STEP_NS = {1: 0.50, 2: 0.714, 3: 1.83, 4: 2.27, 6: 6.49, 8: 8.18}
 # Latency of one step attempt of a system whose warp has an SM sub-partition
 # to itself (us), measured on single systems of the mixed-K workload.
-ALONE_US = {1: 18.0, 2: 20.8, 3: 23.0, 4: 26.0, 6: 31.0, 8: 35.5}
+ALONE_US = {1: 16.0, 2: 18.3, 3: 20.5, 4: 22.4, 6: 27.0, 8: 29.6}
 
 
 def cost_weight(K) -> np.ndarray:
@@ -332,10 +332,10 @@ class Ensemble:
         return Plan(self, max_steps, work)
 
     def adaptive_plan(self, max_steps: int = 1_000_000, slices=(1.0, 2.0, 4.0, 8.0),
-                      max_lane_sms: int = 24) -> "AdaptivePlan":
+                      max_lane_sms: int = 32, load_factor: float = 1.45) -> "AdaptivePlan":
         if not self.dev:
             self.to_device()
-        return AdaptivePlan(self, max_steps, slices, max_lane_sms)
+        return AdaptivePlan(self, max_steps, slices, max_lane_sms, load_factor)
 
     def scheduled_plan(self, max_steps: int = 1_000_000, pilot_steps: int = 2048,
                        latency_lane: bool = True) -> "ScheduledPlan":
@@ -455,7 +455,9 @@ class AdaptivePlan:
     * remaining attempts of a system = its observed attempts per unit of
       simulated time x its remaining span (the median rate of its K while it
       has not run enough steps to measure its own);
-    * a system whose remaining attempts at its alone latency (``ALONE_US``)
+    * a system whose remaining attempts at the latency it sees outside a lane
+      (its alone latency ``ALONE_US`` x ``load_factor``: steady cost per
+      attempt x systems in flight / alone latency = 1.42-1.48 on a full B200)
       exceed the predicted bulk time would end last: it goes to a latency
       lane (an SM of its own, ``cbc_work.exclusive``), longest first, up to
       ``max_lane_sms`` SMs;
@@ -468,11 +470,13 @@ class AdaptivePlan:
 
     MIN_OBSERVED = 256   # attempts before a system's own rate is trusted
 
-    def __init__(self, ens: Ensemble, max_steps: int, slices=(1.0, 2.0, 4.0, 8.0), max_lane_sms: int = 24):
+    def __init__(self, ens: Ensemble, max_steps: int, slices=(1.0, 2.0, 4.0, 8.0), max_lane_sms: int = 32,
+                 load_factor: float = 1.45):
         self.ens = ens
         self.max_steps = int(max_steps)
         self.slices = [float(s) for s in slices]
         self.max_lane_sms = int(max_lane_sms)
+        self.load_factor = float(load_factor)
         self.history: List[dict] = []
         import torch
         self.sm_count = torch.cuda.get_device_properties(ens.device).multi_processor_count
@@ -499,7 +503,7 @@ class AdaptivePlan:
         count: Dict[int, int] = {}
         for s in ids[np.argsort(-serial_s[ids], kind="stable")]:
             rest = self.sm_count - lane_sms
-            if serial_s[s] * 1.1 < bulk_s * self.sm_count / max(rest, 1):
+            if serial_s[s] * self.load_factor < bulk_s * self.sm_count / max(rest, 1):
                 break
             k = int(K[s])
             opens = count.get(k, 0) % (4 * (32 // k)) == 0

@@ -253,6 +253,10 @@ int32_t cbc_ensemble_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_ens
 }
 
 // ---- allocation-free batched solve -------------------------------------
+// For callers that cannot cudaMalloc while they step (their device memory is
+// held by another allocator or a fixed budget).  Host code must not pass
+// g_noalloc_scratch itself to a kernel: in host code the name stands for a
+// host-side shadow; the device address comes from cudaGetSymbolAddress.
 // Scheduling scratch of cbc_ensemble_solve_noalloc: CBC_MAX_BUCKETS work-list
 // cursors, then the epoch word (kScheduleBytes = 144 bytes per device).  The
 // cursors are zeroed by every call on its stream before its kernels run; the

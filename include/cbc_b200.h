@@ -240,7 +240,15 @@ int32_t cbc_ensemble_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_ens
                            const cbc_work* work, int64_t max_steps, void* stream);
 
 /* The same batched solve, allocating nothing: no cudaMalloc / cudaFree and no
- * host heap on success.  Its scheduling scratch (the work-list cursors and
+ * host heap on success.  It is for callers that must not allocate while they
+ * step the ensemble: a training or control loop whose device memory is held
+ * by another allocator (a PyTorch caching allocator that has reserved the
+ * GPU, a fixed per-process memory budget), where a cudaMalloc would fail or
+ * stall the whole device, or code that calls the solver from a place where
+ * allocation is not allowed.  Their buffers (the cbc_ensemble arrays) are
+ * theirs; the solver only needs 144 bytes of its own, which are built into
+ * the library and held by every GPU that loads it until the process exits.
+ * Its scheduling scratch (the work-list cursors and
  * the time-slice epoch, 144 bytes) is a static device array of the library,
  * whose address is looked up once per device (cudaGetSymbolAddress) on the
  * first call with that context's device; make that first call outside any

@@ -1,5 +1,7 @@
-"""cbc_ensemble_solve_noalloc (scheduling scratch in a static device array,
-nothing allocated per call) gives bit-identical results to
+"""cbc_ensemble_solve_noalloc is for callers that cannot allocate device
+memory while they step (their GPU memory belongs to another allocator or a
+fixed budget); its scheduling scratch is a static device array of the
+library, so nothing is allocated per call.  It gives bit-identical results to
 cbc_ensemble_solve, over two calls in a row (the second resumes where the
 first stopped), with and without a time slice.  Kept in its own file, named to
 be collected last, so that it also runs after every other test in one process
