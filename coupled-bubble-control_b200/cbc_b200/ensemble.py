@@ -440,6 +440,52 @@ def lane_work_list(wl: WorkList, K: np.ndarray, lane_ids: np.ndarray, order_key:
                     exclusive=np.asarray(excl, np.int32))
 
 
+def adaptive_work_list(K, t_end, t0, a0, t, attempts, active, sm_count: int, max_lane_sms: int = 32,
+                       load_factor: float = 1.45, min_observed: int = 256):
+    """One re-planning step of ``AdaptivePlan`` (host only): the work list
+    for the systems still running, from the progress since the solve began
+    (t0 / a0: simulated time and step attempts then; t / attempts: now).
+    Returns (work list, summary dict)."""
+    K = np.asarray(K)
+    ids = np.nonzero(active)[0]
+    adv = t - t0
+    obs = attempts - a0
+    own = (obs >= min_observed) & (adv > 0)
+    rate = np.zeros(K.shape[0])
+    rate[own] = obs[own] / adv[own]
+    for k in np.unique(K[ids]):
+        sel = (K == k) & own
+        fill = float(np.median(rate[sel])) if np.any(sel) else 2000.0
+        rate[(K == k) & ~own] = fill
+    remaining = rate * np.maximum(t_end - t, 0.0)
+    serial_s = remaining * alone_latency(K) * 1e-6
+    bulk_s = float(np.sum(remaining[ids] * cost_weight(K[ids]))) * 1e-9
+    wl = make_work_list(K, remaining, active=active)
+    # latency lanes for the systems that would otherwise end last
+    lane_sms = 0
+    picked: List[int] = []
+    sms: Dict[int, int] = {}
+    count: Dict[int, int] = {}
+    for s in ids[np.argsort(-serial_s[ids], kind="stable")]:
+        rest = sm_count - lane_sms
+        if serial_s[s] * load_factor < bulk_s * sm_count / max(rest, 1):
+            break
+        k = int(K[s])
+        opens = count.get(k, 0) % (4 * (32 // k)) == 0
+        if opens and lane_sms + 1 > max_lane_sms:
+            break
+        if opens:
+            sms[k] = sms.get(k, 0) + 1
+            lane_sms += 1
+        count[k] = count.get(k, 0) + 1
+        picked.append(int(s))
+    if picked:
+        wl = lane_work_list(wl, K, np.asarray(picked), serial_s, sms)
+    info = {"active": int(ids.size), "bulk_s": bulk_s, "lane_systems": len(picked), "lane_sms": lane_sms,
+            "max_serial_s": float(serial_s[ids].max()) if ids.size else 0.0}
+    return wl, info
+
+
 class AdaptivePlan:
     """Time-sliced batched solve that re-plans between slices.
 
@@ -482,42 +528,9 @@ class AdaptivePlan:
         self.sm_count = torch.cuda.get_device_properties(ens.device).multi_processor_count
 
     def plan(self, K, t_end, t0, a0, t, attempts, active) -> WorkList:
-        ids = np.nonzero(active)[0]
-        adv = t - t0
-        obs = attempts - a0
-        own = (obs >= self.MIN_OBSERVED) & (adv > 0)
-        rate = np.zeros(K.shape[0])
-        rate[own] = obs[own] / adv[own]
-        for k in np.unique(K[ids]):
-            sel = (K == k) & own
-            fill = float(np.median(rate[sel])) if np.any(sel) else 2000.0
-            rate[(K == k) & ~own] = fill
-        remaining = rate * np.maximum(t_end - t, 0.0)
-        serial_s = remaining * alone_latency(K) * 1e-6
-        bulk_s = float(np.sum(remaining[ids] * cost_weight(K[ids]))) * 1e-9
-        wl = make_work_list(K, remaining, active=active)
-        # latency lanes for the systems that would otherwise end last
-        lane_sms = 0
-        picked: List[int] = []
-        sms: Dict[int, int] = {}
-        count: Dict[int, int] = {}
-        for s in ids[np.argsort(-serial_s[ids], kind="stable")]:
-            rest = self.sm_count - lane_sms
-            if serial_s[s] * self.load_factor < bulk_s * self.sm_count / max(rest, 1):
-                break
-            k = int(K[s])
-            opens = count.get(k, 0) % (4 * (32 // k)) == 0
-            if opens and lane_sms + 1 > self.max_lane_sms:
-                break
-            if opens:
-                sms[k] = sms.get(k, 0) + 1
-                lane_sms += 1
-            count[k] = count.get(k, 0) + 1
-            picked.append(int(s))
-        if picked:
-            wl = lane_work_list(wl, K, np.asarray(picked), serial_s, sms)
-        self.history.append({"active": int(ids.size), "bulk_s": bulk_s, "lane_systems": len(picked),
-                             "lane_sms": lane_sms, "max_serial_s": float(serial_s[ids].max()) if ids.size else 0.0})
+        wl, info = adaptive_work_list(K, t_end, t0, a0, t, attempts, active, self.sm_count, self.max_lane_sms,
+                                      self.load_factor, self.MIN_OBSERVED)
+        self.history.append(info)
         return wl
 
     def launch(self, stream=None) -> None:

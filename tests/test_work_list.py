@@ -24,3 +24,34 @@ def test_latency_lane_work_list():
         seg = wl.order[wl.bucket_begin[b]:wl.bucket_begin[b + 1]]
         assert np.all(K[seg] == k) and seg.size <= ex[b] * 4 * (32 // k)
     assert np.all(wl.share[lanes] == 0)
+
+
+def test_adaptive_replanning_host_logic():
+    """AdaptivePlan's re-planning step: rates from observed progress, the
+    systems that would end last go to latency lanes (longest first, inside
+    the SM budget), every active system appears exactly once, finished ones
+    not at all."""
+    from cbc_b200.ensemble import adaptive_work_list
+    rng = np.random.default_rng(5)
+    n = 3000
+    K = rng.choice([2, 3, 4, 6, 8], size=n)
+    t_end = rng.uniform(5.0, 50.0, n)
+    t0 = np.zeros(n)
+    t = rng.uniform(0.0, 1.0, n)
+    rate = rng.uniform(500, 3000, n)
+    rate[:5] = 12000.0                     # five systems that step very slowly through time
+    attempts = (rate * t).astype(np.int64)
+    a0 = np.zeros(n, np.int64)
+    active = np.ones(n, bool)
+    active[100:200] = False                # finished
+    wl, info = adaptive_work_list(K, t_end, t0, a0, t, attempts, active, sm_count=148, max_lane_sms=8)
+    assert sorted(wl.order.tolist()) == sorted(np.nonzero(active)[0].tolist())
+    assert info["lane_systems"] > 0 and 1 <= info["lane_sms"] <= 8
+    lanes = [b for b in range(wl.bucket_K.size) if wl.exclusive[b] > 0]
+    in_lane = set(np.concatenate([wl.order[wl.bucket_begin[b]:wl.bucket_begin[b + 1]] for b in lanes]).tolist())
+    slow = [i for i in range(5) if t_end[i] * 12000.0 * 1e-6 * 29.6 > 2.0]   # long serial chains
+    assert set(slow) <= in_lane
+    # with no observations yet the fallback rate still yields a complete list
+    # inside the default lane budget of 32 SMs
+    wl2, info2 = adaptive_work_list(K, np.full(n, 0.01), t0, a0, t0, a0, active, sm_count=148)
+    assert sorted(wl2.order.tolist()) == sorted(np.nonzero(active)[0].tolist()) and info2["lane_sms"] <= 32
