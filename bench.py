@@ -175,6 +175,16 @@ def cpu_baseline(scene, seconds: float = 12.0, nthreads: int = 0, seed: int = 99
                       f"(C++ restatement of the reference integrator) on {cores} threads"}
 
 
+def workload_config(args, world: int) -> dict:
+    """The workload both arms report (the reference arm times a bounded CPU
+    sample of it, described in its cpu_baseline.sample)."""
+    return {"workload": f"mixed_k_{args.ns}", "ns_per_gpu": args.ns, "K": [2, 3, 4, 6, 8],
+            "K_weights": [0.4, 0.2, 0.2, 0.1, 0.1], "span_periods": [5, 50], "rtol": 1e-9,
+            "atol": 1e-9, "max_steps": args.max_steps, "field": "SW_A 25+50 kHz",
+            "l2": "256 MiB buffer written before every step", "parallelism": f"replicas{world}",
+            "schedule": args.schedule}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -190,7 +200,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"mixed_k_{args.ns}", "sample": "bounded CPU sample"},
+            "config": workload_config(args, world),
             "cpu_baseline": {**r, "value": v},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -384,11 +394,7 @@ def run_b200(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_all / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"mixed_k_{args.ns}", "ns_per_gpu": args.ns, "K": [2, 3, 4, 6, 8],
-                       "K_weights": [0.4, 0.2, 0.2, 0.1, 0.1], "span_periods": [5, 50], "rtol": 1e-9,
-                       "atol": 1e-9, "max_steps": args.max_steps, "field": "SW_A 25+50 kHz",
-                       "l2": "256 MiB buffer written before every step", "parallelism": f"replicas{world}",
-                       "schedule": args.schedule},
+            "config": workload_config(args, world),
             "work": {"advanced_system_periods_per_step": adv, "nominal_system_periods": float(np.sum(scene.t_end)),
                      "status_counts": status, "steps_per_solve": int(np.sum(res["steps"])),
                      "richardson_sweeps_per_rhs": float(np.sum(res["lin_iters"]) / max(1, 6 * np.sum(res["steps"]))),
