@@ -6,7 +6,8 @@ backend (``CKM1D(...).solve()`` -> ``backends/numba/rkck45_coupled_numba_solver.
 (NUMBA_ENABLE_CUDASIM=1) on the CPU of the build container, and stores the
 initial host buffers together with the reference's final buffers in
 ``golden_ref_numba.npz``.  The reference tree is read from REFERENCE_ROOT
-(default /root/reference); it is not needed anywhere else.
+(default /root/reference); it is not needed anywhere else.  GOLDEN_SET=long or
+GOLDEN_SET=k8 selects the longer-span or the K = 8 cases.
 
 The simulator lacks a few features the reference relies on; these shims are
 applied before importing it and change no arithmetic:
@@ -106,6 +107,14 @@ CASES_LONG = [
 ]
 
 
+# K = 8 (every partner-sum chain of the kernels holds two partners).  Written to
+# golden_ref_numba_k8.npz with GOLDEN_SET=k8.
+CASES_K8 = [
+    ("k8_swa", 8, "SW_A", 2, [5.0, 3.0, 4.0, 6.0, 2.5, 5.5, 3.5, 4.5], [1.1, 0.6], [25.0, 50.0], [0.4, 1.3],
+     [-0.35, -0.25, -0.15, -0.05, 0.05, 0.15, 0.25, 0.35], 0.001),
+]
+
+
 def run_case(case, water):
     from coupledbubble_control.models import CKM1D, MaterialProperties
     from coupledbubble_control.backends import BackendName, KernelVariant
@@ -141,8 +150,9 @@ def main():
     install_shims()
     sys.path.insert(0, REF)
     out = {}
-    long_set = os.environ.get("GOLDEN_SET", "") == "long"
-    for case in (CASES_LONG if long_set else CASES):
+    which = os.environ.get("GOLDEN_SET", "")
+    cases = {"long": CASES_LONG, "k8": CASES_K8}.get(which, CASES)
+    for case in cases:
         print("running", case[0], flush=True)
         init, final, meta = run_case(case, water=True)
         for k, v in init.items():
@@ -151,7 +161,7 @@ def main():
             out[f"{meta['name']}/final/{k}"] = v
         out[f"{meta['name']}/meta"] = np.array([meta["K"], meta["nk"], ["CONST", "SW_N", "SW_A"].index(meta["ac"])])
         print("  t", final["actual_time"], "R", final["actual_state"][0, 0, :meta["K"]], flush=True)
-    fn = os.path.join(HERE, "golden_ref_numba_long.npz" if long_set else "golden_ref_numba.npz")
+    fn = os.path.join(HERE, f"golden_ref_numba_{which}.npz" if which in ("long", "k8") else "golden_ref_numba.npz")
     np.savez_compressed(fn, **out)
     print("wrote", fn)
 
