@@ -7,7 +7,7 @@ backend (``CKM1D(...).solve()`` -> ``backends/numba/rkck45_coupled_numba_solver.
 initial host buffers together with the reference's final buffers in
 ``golden_ref_numba.npz``.  The reference tree is read from REFERENCE_ROOT
 (default /root/reference); it is not needed anywhere else.  GOLDEN_SET=long or
-GOLDEN_SET=k8 selects the longer-span or the K = 8 cases.
+GOLDEN_SET=k8 / k16 selects the longer-span, K = 8 or K = 16 cases.
 
 The simulator lacks a few features the reference relies on; these shims are
 applied before importing it and change no arithmetic:
@@ -115,6 +115,14 @@ CASES_K8 = [
 ]
 
 
+# K = 16 (the generic-K kernel: chains of three and four partners).  Written to
+# golden_ref_numba_k16.npz with GOLDEN_SET=k16.
+CASES_K16 = [
+    ("k16_swa", 16, "SW_A", 2, [4.0 + 0.25 * (i % 7) for i in range(16)], [1.0, 0.5], [25.0, 50.0], [0.2, 0.9],
+     [-0.375 + 0.05 * i for i in range(16)], 0.0005),
+]
+
+
 def run_case(case, water):
     from coupledbubble_control.models import CKM1D, MaterialProperties
     from coupledbubble_control.backends import BackendName, KernelVariant
@@ -151,7 +159,7 @@ def main():
     sys.path.insert(0, REF)
     out = {}
     which = os.environ.get("GOLDEN_SET", "")
-    cases = {"long": CASES_LONG, "k8": CASES_K8}.get(which, CASES)
+    cases = {"long": CASES_LONG, "k8": CASES_K8, "k16": CASES_K16}.get(which, CASES)
     for case in cases:
         print("running", case[0], flush=True)
         init, final, meta = run_case(case, water=True)
@@ -161,7 +169,7 @@ def main():
             out[f"{meta['name']}/final/{k}"] = v
         out[f"{meta['name']}/meta"] = np.array([meta["K"], meta["nk"], ["CONST", "SW_N", "SW_A"].index(meta["ac"])])
         print("  t", final["actual_time"], "R", final["actual_state"][0, 0, :meta["K"]], flush=True)
-    fn = os.path.join(HERE, f"golden_ref_numba_{which}.npz" if which in ("long", "k8") else "golden_ref_numba.npz")
+    fn = os.path.join(HERE, f"golden_ref_numba_{which}.npz" if which in ("long", "k8", "k16") else "golden_ref_numba.npz")
     np.savez_compressed(fn, **out)
     print("wrote", fn)
 
