@@ -103,6 +103,8 @@ CASES = [
 # driven cases).  Written to golden_ref_numba_long.npz with GOLDEN_SET=long.
 CASES_LONG = [
     ("k2_swa_long", 2, "SW_A", 2, [6.0, 4.0], [1.3, 0.8], [25.0, 50.0], [0.7, 1.6], [-0.1, 0.02], 0.06),
+    ("k4_swa_long", 4, "SW_A", 2, [5.0, 3.5, 6.0, 4.0], [1.2, 0.7], [25.0, 50.0], [0.5, 1.4],
+     [-0.2, -0.08, 0.06, 0.18], 0.03),
     ("k2_const_long", 2, "CONST", 1, [7.0, 5.0], [-1.2156], [20.0], [0.0], [0.0, 200e-6 / (1497.0 / 20e3)], 0.06),
 ]
 
