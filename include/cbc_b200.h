@@ -252,7 +252,9 @@ int32_t cbc_ensemble_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_ens
  * the time-slice epoch, 144 bytes) is a static device array of the library,
  * whose address is looked up once per device (cudaGetSymbolAddress) on the
  * first call with that context's device; make that first call outside any
- * stream capture.  The cursors are zeroed by each call on `stream` before its
+ * stream capture.  The looked-up address is kept for the life of the
+ * process: a process that resets a device (cudaDeviceReset) must not call
+ * this entry point on that device afterwards.  The cursors are zeroed by each call on `stream` before its
  * kernels.  Work lists of more than CBC_MAX_BUCKETS buckets are rejected
  * (CBC_E_INVALID from the common checks).  The scratch is shared by all calls
  * on a device: calls whose executions overlap in time (different streams,
