@@ -7,7 +7,8 @@ backend (``CKM1D(...).solve()`` -> ``backends/numba/rkck45_coupled_numba_solver.
 initial host buffers together with the reference's final buffers in
 ``golden_ref_numba.npz``.  The reference tree is read from REFERENCE_ROOT
 (default /root/reference); it is not needed anywhere else.  GOLDEN_SET=long or
-GOLDEN_SET=k8 / k16 selects the longer-span, K = 8 or K = 16 cases.
+GOLDEN_SET=k8 / k16 / fields selects the longer-span, K = 8, K = 16 or
+the SW_N / CONST multi-bubble cases.
 
 The simulator lacks a few features the reference relies on; these shims are
 applied before importing it and change no arithmetic:
@@ -125,6 +126,16 @@ CASES_K16 = [
 ]
 
 
+# SW_N and CONST fields with several coupled bubbles.  Written to
+# golden_ref_numba_fields.npz with GOLDEN_SET=fields.
+CASES_FIELDS = [
+    ("k4_swn", 4, "SW_N", 2, [5.0, 4.0, 6.0, 3.0], [0.6, 0.4], [25.0, 50.0], [0.0, 0.0],
+     [-0.15, -0.05, 0.05, 0.15], 0.002),
+    ("k8_const", 8, "CONST", 1, [7.0, 5.0, 6.0, 4.0, 5.5, 6.5, 4.5, 5.0], [-1.0], [20.0], [0.0],
+     [-0.35, -0.25, -0.15, -0.05, 0.05, 0.15, 0.25, 0.35], 0.001),
+]
+
+
 def run_case(case, water):
     from coupledbubble_control.models import CKM1D, MaterialProperties
     from coupledbubble_control.backends import BackendName, KernelVariant
@@ -161,7 +172,7 @@ def main():
     sys.path.insert(0, REF)
     out = {}
     which = os.environ.get("GOLDEN_SET", "")
-    cases = {"long": CASES_LONG, "k8": CASES_K8, "k16": CASES_K16}.get(which, CASES)
+    cases = {"long": CASES_LONG, "k8": CASES_K8, "k16": CASES_K16, "fields": CASES_FIELDS}.get(which, CASES)
     for case in cases:
         print("running", case[0], flush=True)
         init, final, meta = run_case(case, water=True)
@@ -171,7 +182,7 @@ def main():
             out[f"{meta['name']}/final/{k}"] = v
         out[f"{meta['name']}/meta"] = np.array([meta["K"], meta["nk"], ["CONST", "SW_N", "SW_A"].index(meta["ac"])])
         print("  t", final["actual_time"], "R", final["actual_state"][0, 0, :meta["K"]], flush=True)
-    fn = os.path.join(HERE, f"golden_ref_numba_{which}.npz" if which in ("long", "k8", "k16") else "golden_ref_numba.npz")
+    fn = os.path.join(HERE, f"golden_ref_numba_{which}.npz" if which in ("long", "k8", "k16", "fields") else "golden_ref_numba.npz")
     np.savez_compressed(fn, **out)
     print("wrote", fn)
 

@@ -11,8 +11,9 @@ multiply-adds, the oracle with cbc_math and explicit fma, so they differ at
 the rounding level (~1e-16 per operation).  Over the few hundred steps of a
 case this stays far below the integrator tolerance: we require relative
 agreement 1e-11 on every state component (floor 1e-12 absolute; observed
-<= 8.2e-14 for K = 1, 2, 4, 16 (up to 214 steps); 2.9e-12 for K = 8, where one bubble's dR/dt is
-near a zero crossing: absolute error 9e-15 against |dR/dt| up to 16) and
+<= 8.2e-14 for K = 1, 2, 4, 16 (up to 214 steps; SW_A, SW_N, CONST);
+<= 2.9e-12 for the K = 8 cases, on components near zero (absolute error
+<= 9e-15, against |dR/dt| up to 16)) and
 identical end times and statuses.
 """
 import os
