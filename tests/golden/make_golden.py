@@ -7,8 +7,8 @@ backend (``CKM1D(...).solve()`` -> ``backends/numba/rkck45_coupled_numba_solver.
 initial host buffers together with the reference's final buffers in
 ``golden_ref_numba.npz``.  The reference tree is read from REFERENCE_ROOT
 (default /root/reference); it is not needed anywhere else.  GOLDEN_SET=long or
-GOLDEN_SET=k8 / k16 / fields selects the longer-span, K = 8, K = 16 or
-the SW_N / CONST multi-bubble cases.
+GOLDEN_SET=k8 / k16 / fields / events selects the longer-span, K = 8, K = 16,
+the SW_N / CONST multi-bubble or the collision-event cases.
 
 The simulator lacks a few features the reference relies on; these shims are
 applied before importing it and change no arithmetic:
@@ -136,6 +136,14 @@ CASES_FIELDS = [
 ]
 
 
+# Two bubbles that start just outside the collision threshold and grow into
+# it: event bracketing by step rejection and the terminal status 2.  Written
+# to golden_ref_numba_events.npz with GOLDEN_SET=events.
+CASES_EVENTS = [
+    ("k2_event", 2, "SW_A", 2, [20.0, 20.0], [1.2, 0.1], [25.0, 50.0], [0.75, 0.0], [0.0, 7.548029e-04], 0.1),
+]
+
+
 def run_case(case, water):
     from coupledbubble_control.models import CKM1D, MaterialProperties
     from coupledbubble_control.backends import BackendName, KernelVariant
@@ -172,7 +180,8 @@ def main():
     sys.path.insert(0, REF)
     out = {}
     which = os.environ.get("GOLDEN_SET", "")
-    cases = {"long": CASES_LONG, "k8": CASES_K8, "k16": CASES_K16, "fields": CASES_FIELDS}.get(which, CASES)
+    cases = {"long": CASES_LONG, "k8": CASES_K8, "k16": CASES_K16, "fields": CASES_FIELDS,
+             "events": CASES_EVENTS}.get(which, CASES)
     for case in cases:
         print("running", case[0], flush=True)
         init, final, meta = run_case(case, water=True)
@@ -182,7 +191,8 @@ def main():
             out[f"{meta['name']}/final/{k}"] = v
         out[f"{meta['name']}/meta"] = np.array([meta["K"], meta["nk"], ["CONST", "SW_N", "SW_A"].index(meta["ac"])])
         print("  t", final["actual_time"], "R", final["actual_state"][0, 0, :meta["K"]], flush=True)
-    fn = os.path.join(HERE, f"golden_ref_numba_{which}.npz" if which in ("long", "k8", "k16", "fields") else "golden_ref_numba.npz")
+    fn = os.path.join(HERE, f"golden_ref_numba_{which}.npz" if which in ("long", "k8", "k16", "fields", "events")
+                      else "golden_ref_numba.npz")
     np.savez_compressed(fn, **out)
     print("wrote", fn)
 

@@ -15,6 +15,16 @@ agreement 1e-11 on every state component (floor 1e-12 absolute; observed
 <= 2.9e-12 for the K = 8 cases, on components near zero (absolute error
 <= 9e-15, against |dR/dt| up to 16)) and
 identical end times and statuses.
+
+Cases that end on a collision event (status 2) stop at the first accepted
+step whose collision gap is below ETOL, so their end time depends on the
+exact step grid.  The controller's step sizes follow the embedded error
+estimate, a difference of O(1) stage values at the 1e-9 level whose own
+relative rounding is ~1e-7; a one-ulp change of the initial radius moves the
+oracle's own end state of the k2_event case by 1.8e-8 (end time by
+1.7e-10).  For these cases the bound is the path's stated tolerance, 1e-7
+relative on every state component, with the same status (observed 6.7e-9,
+end times 6.5e-11 apart).
 """
 import os
 
@@ -49,14 +59,17 @@ def test_oracle_matches_reference_numba(name, z):
     spec = oracle.make_spec(ns, K, tile, 0, nk, AC[ac], SolverSpec())
     oracle.solve_ref_layout(spec, buf, 1_000_000)
     assert np.all(buf["status_flags"] == final["status_flags"]), (buf["status_flags"], final["status_flags"])
-    np.testing.assert_allclose(buf["actual_time"], final["actual_time"], rtol=0, atol=1e-15)
+    event_end = bool(np.all(final["status_flags"] == 2))
+    np.testing.assert_allclose(buf["actual_time"], final["actual_time"], rtol=1e-8 if event_end else 0,
+                               atol=0 if event_end else 1e-15)
     a = buf["actual_state"][:, :, :K]
     b = final["actual_state"][:, :, :K]
     err = np.abs(a - b) / np.maximum(np.abs(b), 1e-12)
-    assert np.max(err) < 1e-11, f"max relative state error {np.max(err):.3e}"
+    bound = 1e-7 if event_end else 1e-11
+    assert np.max(err) < bound, f"max relative state error {np.max(err):.3e}"
     # event value (collision gap) agrees to the same level
     if K > 1:
-        np.testing.assert_allclose(buf["actual_event"], final["actual_event"], rtol=1e-9)
+        np.testing.assert_allclose(buf["actual_event"], final["actual_event"], rtol=1e-6 if event_end else 1e-9)
 
 
 def test_golden_file_present():
