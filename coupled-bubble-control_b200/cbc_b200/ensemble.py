@@ -160,10 +160,6 @@ def with_latency_lane(wl: WorkList, K: np.ndarray, work: np.ndarray, fraction: f
 class Ensemble:
     """Ragged ensemble: host numpy arrays plus torch device copies."""
 
-    FIELDS_F64 = ("state", "unit_params", "system_params", "control_params", "coupling", "t", "t_end",
-                  "t_begin", "h", "event")
-    FIELDS_I32 = ("status", "dense_index", "steps", "rejected", "conv_ok", "conv_fail")
-
     def __init__(self, host: Dict[str, np.ndarray], nk: int, ac: str, ndo: int,
                  solver_spec: Optional[SolverSpec] = None, device: int = 0):
         self.host = host
