@@ -1,9 +1,10 @@
 """Compile-option record accepted by ``CKM1D(...)``.
 
 Same fields and mode semantics as ``coupledbubble_control/backends/cuda_opts.py``
-(:6-73).  The B200 library is built ahead of time for sm_100a, so these options
-do not recompile anything; they are kept so that constructors written for the
-reference work unchanged, and ``mode`` is reported back in ``debug`` output.
+(:6-73).  The B200 library is built ahead of time for sm_100a, so nothing
+reads this record: ``CKM1D(...)`` stores it only so that constructors written
+for the reference (``compiler=``, ``max_registers=``, ``fastmath=``,
+``cuda_mode=``) keep working unchanged.
 """
 from dataclasses import dataclass
 from typing import Literal, Optional

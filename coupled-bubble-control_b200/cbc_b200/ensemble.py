@@ -269,12 +269,18 @@ class Ensemble:
             e.dense_state = d["dense_state"].data_ptr()
         return e
 
-    def work(self, wl: Optional[WorkList] = None, budget_ns: int = 0, steps_total: bool = False):
-        """(cbc_work, keep-alive list) for a work list (default: all systems)."""
+    def work(self, wl: Optional[WorkList] = None, budget_ns: int = 0, steps_total: bool = False, stream=None):
+        """(cbc_work, keep-alive list) for a work list (default: all systems).
+        The device copy of the order is made on `stream` (default: the current
+        torch stream), so kernels later enqueued on that stream see it, and is
+        marked in use by that stream for torch's caching allocator."""
         import torch
         if wl is None:
             wl = make_work_list(self.host["K"], self.host["t_end"] - self.host["t"])
-        order = torch.from_numpy(wl.order).to(torch.device("cuda", self.device))
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.stream(st):
+            order = torch.from_numpy(wl.order).to(torch.device("cuda", self.device), non_blocking=False)
+        order.record_stream(st)
         keep = [order, wl]
         w = _lib.cbc_work()
         w.order = order.data_ptr()
@@ -316,8 +322,8 @@ class Ensemble:
             self.to_device()
         ctx = _lib.default_context(self.device)
         spec, e = self.spec(), self.abi()
-        w, keep = self.work(work, budget_ns, steps_total)
         st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        w, keep = self.work(work, budget_ns, steps_total, stream=st)
         ctx.check(_lib.lib().cbc_ensemble_solve(ctx.handle, ctypes.byref(spec), ctypes.byref(e),
                                                 ctypes.byref(w), int(max_steps), ctypes.c_void_p(st.cuda_stream)))
         self._keep = keep
@@ -368,6 +374,12 @@ class ScheduledPlan:
         self.latency_lane = bool(latency_lane)
 
     def launch(self, stream=None) -> None:
+        import torch
+        st = stream if stream is not None else torch.cuda.current_stream(self.ens.device)
+        with torch.cuda.stream(st):   # every torch op of the plan is ordered with its kernels
+            self._launch(st)
+
+    def _launch(self, stream) -> None:
         import torch
         d = self.ens.dev
         t_start = d["t"].clone()
@@ -531,6 +543,12 @@ class AdaptivePlan:
 
     def launch(self, stream=None) -> None:
         import torch
+        st = stream if stream is not None else torch.cuda.current_stream(self.ens.device)
+        with torch.cuda.stream(st):   # reads, timing events and solves all on one stream
+            self._launch(st)
+
+    def _launch(self, stream) -> None:
+        import torch
         ens, d = self.ens, self.ens.dev
         K = ens.host["K"]
         t_end = d["t_end"].cpu().numpy()
@@ -567,6 +585,8 @@ class Plan:
         self.ctx = _lib.default_context(ens.device)
         self._spec, self._e = ens.spec(), ens.abi()
         self._w, self._keep = ens.work(work)
+        import torch
+        torch.cuda.synchronize(ens.device)   # the order upload is complete before any replay, on any stream
         h = _lib.P()
         self.ctx.check(_lib.lib().cbc_plan_create(self.ctx.handle, ctypes.byref(self._spec), ctypes.byref(self._e),
                                                   ctypes.byref(self._w), int(max_steps), ctypes.byref(h)))

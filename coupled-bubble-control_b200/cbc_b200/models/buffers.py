@@ -1,7 +1,7 @@
 """Host/device buffer sets of the CKM1D integrator.
 
-Mirrors ``coupledbubble_control/models/buffers.py`` (Buffer classes :314-356,
-BufferOps :359-485): the same groups, field names, shapes and in-place
+Mirrors ``coupledbubble_control/models/buffers.py`` (buffer dataclasses
+:29-71, BufferOps :74-200): the same groups, field names, shapes and in-place
 semantics.  Device arrays are ``torch`` CUDA tensors instead of cupy/numba
 arrays; the B200 library only ever sees their raw device pointers.
 

@@ -56,8 +56,6 @@ static int32_t check_ensemble(cbc_context* ctx, const cbc_spec* spec, const cbc_
   if (w->budget_ns < 0) return fail(ctx, CBC_E_INVALID, "budget_ns must be >= 0");
   if (w->steps_total != 0 && w->steps_total != 1) return fail(ctx, CBC_E_INVALID, "steps_total must be 0 or 1");
   if (w->steps_total && !e->steps) return fail(ctx, CBC_E_INVALID, "steps_total needs ensemble.steps");
-  for (int b = 0; b < w->nbuckets; ++b) {
-  }
   return CBC_OK;
 }
 
@@ -268,6 +266,33 @@ constexpr int kNoallocMaxDevices = 64;
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_ptr[kNoallocMaxDevices] = {};
 
+}  // extern "C"
+
+namespace cbc {
+
+// Device address of g_noalloc_scratch on `device`, looked up once per device
+// (cudaGetSymbolAddress, which also loads this file's module on that device)
+// and cached for the life of the process.  Called by cbc_create with the
+// device current, so that cbc_ensemble_solve_noalloc itself never loads the
+// module for the scratch.
+cudaError_t noalloc_scratch_address(int device, void** out) {
+  *out = nullptr;
+  if (device < 0 || device >= kNoallocMaxDevices) return cudaSuccess;  // entry point reports it
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (ce != cudaSuccess) return ce;
+    g_noalloc_ptr[device] = p;
+  }
+  *out = g_noalloc_ptr[device];
+  return cudaSuccess;
+}
+
+}  // namespace cbc
+
+extern "C" {
+
 int32_t cbc_ensemble_solve_noalloc(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e,
                                    const cbc_work* w, int64_t max_steps, void* stream) {
   if (!ctx) return fail(nullptr, CBC_E_INVALID, "context is NULL");
@@ -275,25 +300,12 @@ int32_t cbc_ensemble_solve_noalloc(cbc_context* ctx, const cbc_spec* spec, const
   int32_t rc = check_ensemble(ctx, spec, e, w);
   if (rc) return rc;
   if (max_steps < 1) return fail(ctx, CBC_E_INVALID, "max_steps must be >= 1");
-  if (w->nbuckets > CBC_MAX_BUCKETS)
-    return fail(ctx, CBC_E_UNSUPPORTED, "cbc_ensemble_solve_noalloc: %d buckets exceed its static scratch of %d",
-                w->nbuckets, CBC_MAX_BUCKETS);
   if (ctx->device < 0 || ctx->device >= kNoallocMaxDevices)
     return fail(ctx, CBC_E_UNSUPPORTED, "cbc_ensemble_solve_noalloc: device %d beyond %d", ctx->device,
                 kNoallocMaxDevices);
+  void* scratch = ctx->noalloc_scratch;
+  if (!scratch) return fail(ctx, CBC_E_CUDA, "cbc_ensemble_solve_noalloc: static scratch address unavailable");
   DeviceGuard dg(ctx->device);
-  void* scratch = nullptr;
-  {
-    // set-up once per device, with the device current
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[ctx->device]) {
-      void* p = nullptr;
-      const cudaError_t ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (ce != cudaSuccess || !p) return fail(ctx, CBC_E_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(ce));
-      g_noalloc_ptr[ctx->device] = p;
-    }
-    scratch = g_noalloc_ptr[ctx->device];
-  }
   const auto grids = grid_sizes<GridsT<FixedVec>>(ctx, spec, w);
   return enqueue(ctx, spec, e, w, grids, max_steps, static_cast<int*>(scratch), (cudaStream_t)stream);
 }

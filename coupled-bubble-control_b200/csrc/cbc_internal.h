@@ -30,6 +30,7 @@ struct cbc_context {
   cudaStream_t side[CBC_SIDE_STREAMS] = {};
   cudaStream_t capture = nullptr;  // stream used to capture plans into graphs
   long long launches = 0;          // kernels enqueued (plans: per replay)
+  void* noalloc_scratch = nullptr; // device address of the static scratch of cbc_ensemble_solve_noalloc
   std::string err;
 };
 
@@ -119,6 +120,11 @@ inline int32_t check_spec(cbc_context* ctx, const cbc_spec* s) {
 // bucket) followed by the epoch word (device clock at the solve's start).
 constexpr size_t kHeadBytes = sizeof(int) * CBC_MAX_BUCKETS;
 constexpr size_t kScheduleBytes = kHeadBytes + 2 * sizeof(long long);
+
+// Device address of the static scheduling scratch of
+// cbc_ensemble_solve_noalloc on `device` (which must be current); looked up
+// once per device.  *out stays NULL for device ordinals beyond its table.
+cudaError_t noalloc_scratch_address(int device, void** out);
 
 // Smallest power-of-two instantiation that holds K bubbles per system.
 inline int kb_for(int K) {

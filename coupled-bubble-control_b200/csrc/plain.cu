@@ -192,6 +192,7 @@ int32_t cbc_create(cbc_context** out, int32_t device) {
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ctx->side[i], cudaStreamNonBlocking, prio);
   }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->capture, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = noalloc_scratch_address(device, &ctx->noalloc_scratch);
   cudaSetDevice(prev);
   if (e != cudaSuccess) {
     cbc_destroy(ctx);

@@ -60,8 +60,8 @@ int32_t enqueue_env_begin(cbc_context* ctx, const cbc_ensemble* e, const cbc_env
   const int blocks = (e->ns + threads - 1) / threads;
   ++ctx->launches;
   env_begin_kernel<<<blocks, threads, 0, st>>>(e->ns, io->actions, io->n_act, io->act_stride, io->act_scale,
-                                                const_cast<double*>(e->control_params), e->cp_stride, e->t,
-                                                const_cast<double*>(e->t_end), e->h, e->event, e->status,
+                                                e->control_params, e->cp_stride, e->t,
+                                                e->t_end, e->h, e->event, e->status,
                                                 io->t_span, io->h0);
   CBC_CUDA_TRY(ctx, cudaGetLastError());
   return CBC_OK;

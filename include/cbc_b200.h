@@ -72,7 +72,7 @@ typedef struct cbc_spec {
 } cbc_spec;
 
 /* Device buffers in the reference layout (models/model.py:56-106,
- * models/buffers.py:314-356), mutated in place.  Shapes, row-major:
+ * models/buffers.py:29-71), mutated in place.  Shapes, row-major:
  *   actual_time, time_end, time_begin, time_step, actual_event   (ns)        f64
  *   actual_state                                                 (4, ns, tile) f64  R, X, U, V
  *   unit_params                                                  (13, ns, tile) f64
@@ -161,7 +161,10 @@ int32_t cbc_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_buffers* buf
  *   dense_state                      (ndo, nb, 4)    sample-major; 16-byte aligned
  *   steps, rejected, conv_ok, conv_fail (ns) i32, lin_iters (ns) i64: optional
  * The spec's ns, ups and tile fields are ignored; its solver fields, nk, ac,
- * ndo and dense_mode apply to every system. */
+ * ndo and dense_mode apply to every system.  The solvers only read
+ * control_params and t_end; a plan made by cbc_env_plan_create also writes
+ * them (the actions and the step's end time, see cbc_env_io), which is why
+ * they are not const. */
 typedef struct cbc_ensemble {
   int32_t ns;
   int32_t up_stride, sp_stride, cp_stride;
@@ -171,10 +174,10 @@ typedef struct cbc_ensemble {
   double* state;
   const double* unit_params;
   const double* system_params;
-  const double* control_params;
+  double* control_params;
   const double* coupling;
   double* t;
-  const double* t_end;
+  double* t_end;
   const double* t_begin;
   double* h;
   double* event;
@@ -248,18 +251,20 @@ int32_t cbc_ensemble_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_ens
  * allocation is not allowed.  Their buffers (the cbc_ensemble arrays) are
  * theirs; the solver only needs 144 bytes of its own, which are built into
  * the library and held by every GPU that loads it until the process exits.
- * Its scheduling scratch (the work-list cursors and
- * the time-slice epoch, 144 bytes) is a static device array of the library,
- * whose address is looked up once per device (cudaGetSymbolAddress) on the
- * first call with that context's device; make that first call outside any
- * stream capture.  The looked-up address is kept for the life of the
- * process: a process that resets a device (cudaDeviceReset) must not call
- * this entry point on that device afterwards.  The cursors are zeroed by each call on `stream` before its
- * kernels.  Work lists of more than CBC_MAX_BUCKETS buckets are rejected
- * (CBC_E_INVALID from the common checks).  The scratch is shared by all calls
- * on a device: calls whose executions overlap in time (different streams,
- * no ordering between them) race on it and must not be issued.  No
- * counterpart in the reference. */
+ * Its scheduling scratch (the work-list cursors and the time-slice epoch,
+ * 144 bytes) is a static device array of the library.  Its device address is
+ * looked up (cudaGetSymbolAddress) once per device by cbc_create, with that
+ * device current, and kept for the life of the process: a process that
+ * resets a device (cudaDeviceReset) must not call this entry point on that
+ * device afterwards.  With CUDA's lazy module loading (the default), the
+ * first launch of each bucket kernel on a device loads that kernel, which
+ * may allocate driver memory: make one warm-up call per K bucket shape before
+ * the region that must not allocate (or run with CUDA_MODULE_LOADING=EAGER).
+ * The cursors are zeroed by each call on `stream` before its kernels.  Work
+ * lists of more than CBC_MAX_BUCKETS (32) buckets are rejected with
+ * CBC_E_INVALID.  The scratch is shared by all calls on a device: calls whose
+ * executions overlap in time (different streams, no ordering between them)
+ * race on it and must not be issued.  No counterpart in the reference. */
 int32_t cbc_ensemble_solve_noalloc(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* ens,
                                    const cbc_work* work, int64_t max_steps, void* stream);
 

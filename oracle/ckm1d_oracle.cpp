@@ -23,6 +23,8 @@
 //     schedule continues across relaunches instead of forcing a sample at
 //     every launch (stepper.py:196).  Optional "grid" mode clamps steps so
 //     samples land exactly on t_begin + k (t_end - t_begin)/(NDO-1).
+//     dense_mode 2 (oracle only, for pinning against the reference's own
+//     dense output) replays the reference's behaviour, defect included.
 //   * failure statuses that the reference defines but never sets
 //     (stepper.py:27-33): -4 on a non-finite candidate state; -2 (or -3 when
 //     the implicit coupling iteration failed in that step) when a step at the
@@ -368,23 +370,28 @@ void integrate(System& s, const Spec& sp, double& t, double t_end, double t_begi
   d.t_begin = t_begin;
   d.t_end = t_end;
   d.dt = (sp.ndo == 1) ? (t_end - t_begin) : (sp.ndo > 1 ? (t_end - t_begin) / (double)(sp.ndo - 1) : 0.0);
-  if (sp.dense_mode == 0) {
+  // slot the reference keeps overwriting (dense_mode 2 only; -1 = none)
+  int defect_slot = -1;
+  if (sp.dense_mode == 0 || sp.dense_mode == 2) {
     // reference schedule: next sample = previous stored time + dt, clipped to t_end;
-    // the very first sample is taken at once.
-    if (d.idx == 0 || dense_time_prev == nullptr) d.next = t;
+    // the very first sample is taken at once.  The emulation of the reference
+    // (mode 2) forces a sample at every launch, as its prologue does
+    // (stepper.py:197-200: next sample time = actual time).
+    if (d.idx == 0 || dense_time_prev == nullptr || sp.dense_mode == 2) d.next = t;
     else {
       const double nx = *dense_time_prev + d.dt;
       d.next = nx < t_end ? nx : t_end;
     }
     if (d.idx < d.ndo && d.next <= t) {
-      store(d.idx, t, y);
+      store(d.idx, t, y, true);
+      defect_slot = d.idx;
       d.idx += 1;
       const double nx = t + d.dt;
       d.next = nx < t_end ? nx : t_end;
     }
   } else if (d.ndo > 0) {
     if (d.idx < d.ndo && t >= grid_time(d, d.idx)) {
-      store(d.idx, t, y);
+      store(d.idx, t, y, true);
       d.idx += 1;
     }
   }
@@ -511,13 +518,26 @@ void integrate(System& s, const Spec& sp, double& t, double t_end, double t_begi
     // dense output (stepper.py:634-645, with the slot defect fixed)
     if (sp.dense_mode == 0) {
       if (d.idx < d.ndo && d.next <= t) {
-        store(d.idx, t, y);
+        store(d.idx, t, y, true);
         d.idx += 1;
         const double nx = t + d.dt;
         d.next = nx < t_end ? nx : t_end;
       }
+    } else if (sp.dense_mode == 2) {
+      // the reference as it is (stepper.py:71-112): a new slot takes the time
+      // and the state, and every later step rewrites the state of the last
+      // slot taken, because its store flag is never reset
+      if (d.idx < d.ndo && d.next <= t) {
+        store(d.idx, t, y, true);
+        defect_slot = d.idx;
+        d.idx += 1;
+        const double nx = t + d.dt;
+        d.next = nx < t_end ? nx : t_end;
+      } else if (defect_slot >= 0) {
+        store(defect_slot, t, y, false);
+      }
     } else if (ok && landing) {
-      store(d.idx, t, y);
+      store(d.idx, t, y, true);
       d.idx += 1;
     }
 
@@ -617,9 +637,9 @@ int cbo_solve_ref_layout(const cbo_spec* spec, double* actual_time, const double
     int didx = dense_index ? dense_index[g] : 0;
     const double* prev = (dense_time && didx > 0) ? &dense_time[(size_t)(didx - 1) * NS + g] : nullptr;
     Counters cnt;
-    auto store = [&](int slot, double ts, const double (*yy)[4]) {
+    auto store = [&](int slot, double ts, const double (*yy)[4], bool write_time) {
       if (!dense_time || !dense_state) return;
-      dense_time[(size_t)slot * NS + g] = ts;
+      if (write_time) dense_time[(size_t)slot * NS + g] = ts;
       for (int c = 0; c < 4; ++c)
         for (int i = 0; i < K; ++i) dense_state[((size_t)slot * 4 + c) * NST + (size_t)g * T + i] = yy[i][c];
     };

@@ -13,7 +13,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _AC = {"CONST": 0, "SW_N": 1, "SW_A": 2}
-_DENSE = {"reference": 0, "grid": 1}
+# "reference_defect" (oracle only): the reference's dense output as it is,
+# with its slot overwrite, for pinning against the reference's own samples
+_DENSE = {"reference": 0, "grid": 1, "reference_defect": 2}
 
 
 class cbo_spec(ctypes.Structure):

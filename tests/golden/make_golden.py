@@ -5,8 +5,9 @@ backend (``CKM1D(...).solve()`` -> ``backends/numba/rkck45_coupled_numba_solver.
 -> ``rkck45_coupled_numba_stepper.make_kernel``) under numba's CUDA simulator
 (NUMBA_ENABLE_CUDASIM=1) on the CPU of the build container, and stores the
 initial host buffers together with the reference's final buffers in
-``golden_ref_numba.npz``.  The reference tree is read from REFERENCE_ROOT
-(default /root/reference); it is not needed anywhere else.  GOLDEN_SET=long or
+``golden_ref_numba.npz``.  The reference tree (a checkout of the reference
+repository) is read from the REFERENCE_ROOT environment variable, which must
+be set; it is not needed anywhere else.  GOLDEN_SET=long or
 GOLDEN_SET=k8 / k16 / fields / events selects the longer-span, K = 8, K = 16,
 the SW_N / CONST multi-bubble or the collision-event cases.
 
@@ -34,7 +35,7 @@ os.environ["NUMBA_ENABLE_CUDASIM"] = "1"
 
 import numpy as np  # noqa: E402
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -144,10 +145,33 @@ CASES_EVENTS = [
 ]
 
 
+# Dense output (an 11th field: the number of stored points).  The reference
+# keeps writing the current state into the last stored slot until the next
+# slot is due (its slot flag is never reset), so its dense_state[i] holds the
+# last state before sample i+1 was taken, and the last slot the final state;
+# tests/test_oracle_golden.py replays that rule in the oracle's test-only
+# emulation mode.  Written to golden_ref_numba_dense.npz with GOLDEN_SET=dense.
+CASES_DENSE = [
+    ("k2_swa_dense", 2, "SW_A", 2, [5.0, 3.0], [1.2, 0.4], [25.0, 50.0], [0.3, 1.1], [-0.05, 0.05], 0.004, 5),
+    ("k4_swa_dense", 4, "SW_A", 2, [4.0, 6.0, 3.0, 5.0], [0.9, 0.7], [25.0, 50.0], [1.5, 0.2],
+     [-0.2, -0.1, 0.05, 0.2], 0.002, 4),
+]
+
+
+# A longer span that runs through a bubble collapse (R: 1 -> 3.65 -> 0.18 ->
+# 2.3, about 1,650 steps) with dense output.  Written to
+# golden_ref_numba_collapse.npz with GOLDEN_SET=collapse (a few hours under the
+# simulator).
+CASES_COLLAPSE = [
+    ("k2_collapse", 2, "SW_A", 2, [8.0, 7.5], [1.2, 0.2], [25.0, 50.0], [0.25, 0.0], [-0.1, 0.02], 0.9, 10),
+]
+
+
 def run_case(case, water):
     from coupledbubble_control.models import CKM1D, MaterialProperties
     from coupledbubble_control.backends import BackendName, KernelVariant
-    name, K, ac, nk, R0, PA, FR, PS, X0, t_end = case
+    name, K, ac, nk, R0, PA, FR, PS, X0, t_end = case[:10]
+    ndo = case[10] if len(case) > 10 else 0
     ns = 1
     mp = MaterialProperties()
     if water:
@@ -157,7 +181,7 @@ def run_case(case, water):
                   R0=np.array([R0], dtype=np.float64), PA=np.array(PA, dtype=np.float64)[:, None],
                   FR=np.array(FR, dtype=np.float64)[:, None], PS=np.array(PS, dtype=np.float64)[:, None],
                   REF_FREQ=FR[0], num_components=nk, acoustic_field=ac, mat_props=mp,
-                  backend=BackendName.NUMBA, variant=KernelVariant.SHARED, num_stored_points=0)
+                  backend=BackendName.NUMBA, variant=KernelVariant.SHARED, num_stored_points=ndo)
     hb = model.runtime.host_buffers
     hb.state.time_end[:] = t_end
     hb.state.actual_state[1, :, :K] = np.array(X0)
@@ -168,20 +192,23 @@ def run_case(case, water):
     model.solve(max_steps=1_000_000, kernel_steps=1_000_000, sync_to_host=True)
     final = {}
     db = model.runtime.device_buffers
-    for grp_name in ("state", "status"):
+    for grp_name in ("state", "status") + (("dense",) if ndo > 0 else ()):
         grp = getattr(db, grp_name)
         for k in grp.__dataclass_fields__:
             final[k] = np.array(grp.__getattribute__(k).copy_to_host(), copy=True)
-    return init, final, dict(name=name, K=K, ac=ac, nk=nk)
+    return init, final, dict(name=name, K=K, ac=ac, nk=nk, ndo=ndo)
 
 
 def main():
+    if not REF or not os.path.isdir(REF):
+        raise SystemExit("set REFERENCE_ROOT to a checkout of the reference repository")
     install_shims()
     sys.path.insert(0, REF)
     out = {}
     which = os.environ.get("GOLDEN_SET", "")
-    cases = {"long": CASES_LONG, "k8": CASES_K8, "k16": CASES_K16, "fields": CASES_FIELDS,
-             "events": CASES_EVENTS}.get(which, CASES)
+    sets = {"long": CASES_LONG, "k8": CASES_K8, "k16": CASES_K16, "fields": CASES_FIELDS,
+            "events": CASES_EVENTS, "dense": CASES_DENSE, "collapse": CASES_COLLAPSE}
+    cases = sets.get(which, CASES)
     for case in cases:
         print("running", case[0], flush=True)
         init, final, meta = run_case(case, water=True)
@@ -190,9 +217,9 @@ def main():
         for k, v in final.items():
             out[f"{meta['name']}/final/{k}"] = v
         out[f"{meta['name']}/meta"] = np.array([meta["K"], meta["nk"], ["CONST", "SW_N", "SW_A"].index(meta["ac"])])
+        out[f"{meta['name']}/ndo"] = np.array([meta["ndo"]])
         print("  t", final["actual_time"], "R", final["actual_state"][0, 0, :meta["K"]], flush=True)
-    fn = os.path.join(HERE, f"golden_ref_numba_{which}.npz" if which in ("long", "k8", "k16", "fields", "events")
-                      else "golden_ref_numba.npz")
+    fn = os.path.join(HERE, f"golden_ref_numba_{which}.npz" if which in sets else "golden_ref_numba.npz")
     np.savez_compressed(fn, **out)
     print("wrote", fn)
 

@@ -5,7 +5,9 @@ library, so nothing is allocated per call.  It gives bit-identical results to
 cbc_ensemble_solve, over two calls in a row (the second resumes where the
 first stopped), with and without a time slice.  Kept in its own file, named to
 be collected last, so that it also runs after every other test in one process
-(the scratch address is looked up once per device and then reused)."""
+(the scratch address is looked up once per device, by cbc_create, and then
+reused).  A further test checks the claim itself: over warm calls, free
+device memory and the torch allocator's counters do not move."""
 import ctypes
 
 import numpy as np
@@ -86,4 +88,38 @@ def test_noalloc_rejects_too_many_buckets(cuda):
                                                10, None)
     assert rc == -1
     assert b"bucket" in _lib.lib().cbc_last_error(ctx.handle)
+    del keep
+
+
+def test_noalloc_warm_calls_allocate_nothing(cuda):
+    """After one warm-up call (which may load the bucket kernels lazily), ten
+    more calls leave the device's free memory and torch's allocator counters
+    exactly where they were.  The ABI structures and the work list are built
+    once, outside the measured region, as an allocation-free caller would."""
+    import torch
+    sc = scenes.mixed_k(ns=200, span=(0.2, 0.4), seed=34)
+    ens = Ensemble.from_scene(sc).to_device()
+    ctx = _lib.default_context(ens.device)
+    spec, e = ens.spec(), ens.abi()
+    w, keep = ens.work(make_work_list(ens.host["K"], ens.host["t_end"] - ens.host["t"]))
+    st = torch.cuda.current_stream(ens.device)
+    fn = _lib.lib().cbc_ensemble_solve_noalloc
+
+    def call():
+        ctx.check(fn(ctx.handle, ctypes.byref(spec), ctypes.byref(e), ctypes.byref(w), 40,
+                     ctypes.c_void_p(st.cuda_stream)))
+
+    call()
+    torch.cuda.synchronize(ens.device)
+    free0, _ = torch.cuda.mem_get_info(ens.device)
+    stats0 = torch.cuda.memory_stats(ens.device)
+    for _ in range(10):
+        call()
+    torch.cuda.synchronize(ens.device)
+    free1, _ = torch.cuda.mem_get_info(ens.device)
+    stats1 = torch.cuda.memory_stats(ens.device)
+    assert free1 == free0
+    for k in ("allocation.all.allocated", "segment.all.allocated", "reserved_bytes.all.current"):
+        assert stats1.get(k, 0) == stats0.get(k, 0), k
+    assert np.all(ens.dev["steps"].cpu().numpy() > 0)
     del keep
