@@ -25,13 +25,15 @@ MAX_STEPS_REACHED, STEP_SIZE_LIMIT, CONVERGENCE_FAILURE, SINGULARITY_OR_NAN = -1
 LAUNCH_RELAUNCH, LAUNCH_SINGLE = 0, 1
 AC_CODES = {"CONST": 0, "SW_N": 1, "SW_A": 2}
 DENSE_CODES = {"reference": 0, "grid": 1}
+LIN_CODES = {"richardson": 0, "lu": 1}
 
 
 class cbc_spec(ctypes.Structure):
     _fields_ = [("ns", i32), ("ups", i32), ("tile", i32), ("ndo", i32), ("nk", i32), ("ac", i32),
                 ("dense_mode", i32), ("lin_max_iter", i32), ("atol", f64), ("rtol", f64),
                 ("min_step", f64), ("max_step", f64), ("lin_atol", f64), ("lin_rtol", f64),
-                ("lin_relaxation", f64), ("etol", f64), ("col_threshold", f64)]
+                ("lin_relaxation", f64), ("etol", f64), ("col_threshold", f64), ("lin_solver", i32),
+                ("reserved", i32)]
 
 
 class cbc_buffers(ctypes.Structure):

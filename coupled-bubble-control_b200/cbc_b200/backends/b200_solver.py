@@ -39,7 +39,7 @@ def make_cbc_spec(model_spec, execution_spec, solver_spec) -> _lib.cbc_spec:
         int(model_spec.nk), _lib.AC_CODES[model_spec.ac], _lib.DENSE_CODES[getattr(s, "dense_mode", "reference")],
         int(s.lin_max_iter), float(s.atol), float(s.rtol), float(s.min_step), float(s.max_step),
         float(s.lin_atol), float(s.lin_rtol), float(s.lin_relaxation), float(s.etol),
-        float(getattr(s, "col_threshold", 0.1)))
+        float(getattr(s, "col_threshold", 0.1)), _lib.LIN_CODES[getattr(s, "lin_solver", "richardson")], 0)
 
 
 def load_kernel(model_spec, execution_spec, solver_spec, launch_mode: str = "relaunch") -> KernelHandle:

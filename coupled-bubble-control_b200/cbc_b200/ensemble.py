@@ -249,7 +249,8 @@ class Ensemble:
         s = self.solver_spec
         return _lib.cbc_spec(self.ns, 0, 0, self.ndo, self.nk, _lib.AC_CODES[self.ac],
                              _lib.DENSE_CODES[s.dense_mode], int(s.lin_max_iter), s.atol, s.rtol, s.min_step,
-                             s.max_step, s.lin_atol, s.lin_rtol, s.lin_relaxation, s.etol, s.col_threshold)
+                             s.max_step, s.lin_atol, s.lin_rtol, s.lin_relaxation, s.etol, s.col_threshold,
+                             _lib.LIN_CODES[s.lin_solver], 0)
 
     def abi(self) -> _lib.cbc_ensemble:
         d = self.dev

@@ -75,6 +75,14 @@ class SolverSpec:
     # additions (defaults reproduce the reference kernels)
     col_threshold: float = 0.1            # collision gap factor is (1 + col_threshold)
     dense_mode: Literal["reference", "grid"] = "reference"
+    # implicit-coupling solver: "richardson" (the reference's relaxed
+    # iteration, lin_* fields above) or "lu" (direct solve by Gauss-Jordan
+    # elimination with partial pivoting; exact to rounding, never iterates)
+    lin_solver: Literal["richardson", "lu"] = "richardson"
+
+    def __post_init__(self):
+        if self.lin_solver not in ("richardson", "lu"):
+            raise ValueError(f"lin_solver must be 'richardson' or 'lu', got {self.lin_solver!r}")
 
 
 @dataclass(frozen=True)

@@ -28,6 +28,8 @@ static int32_t check_ensemble(cbc_context* ctx, const cbc_spec* spec, const cbc_
   if (spec->ac < 0 || spec->ac > 2) return fail(ctx, CBC_E_INVALID, "ac = %d out of range", spec->ac);
   if (spec->ndo < 0 || spec->dense_mode < 0 || spec->dense_mode > 1 || spec->lin_max_iter < 0)
     return fail(ctx, CBC_E_INVALID, "ndo, dense_mode or lin_max_iter out of range");
+  if (spec->lin_solver != CBC_LIN_RICHARDSON && spec->lin_solver != CBC_LIN_LU)
+    return fail(ctx, CBC_E_INVALID, "lin_solver = %d: expected 0 (Richardson) or 1 (direct)", spec->lin_solver);
   if (!(spec->min_step > 0.0) || !(spec->max_step >= spec->min_step) || !(spec->atol > 0.0))
     return fail(ctx, CBC_E_INVALID, "need 0 < min_step <= max_step and atol > 0");
   if (!e || !w) return fail(ctx, CBC_E_INVALID, "ensemble or work list is NULL");
@@ -150,7 +152,8 @@ static G grid_sizes(cbc_context* ctx, const cbc_spec* spec, const cbc_work* w) {
     if (n < 1) continue;
     g.exclusive[b] = 1;
     g.first[b] = n;
-    g.threads[b] = kExclusiveThreads;
+    g.threads[b] = block_threads_for(w->bucket_K[b], spec->nk, spec->lin_solver, max_block_smem(ctx->device),
+                                     kExclusiveThreads);
     g.smem[b] = max_block_smem(ctx->device);
     excl_sms += n;
   }
@@ -159,9 +162,10 @@ static G grid_sizes(cbc_context* ctx, const cbc_spec* spec, const cbc_work* w) {
     const int begin = w->bucket_begin[b], end = w->bucket_begin[b + 1];
     if (end <= begin || g.exclusive[b]) continue;
     const int K = w->bucket_K[b];
-    const int threads = w->threads ? w->threads[b] : kDefaultThreads;
+    const int threads = block_threads_for(K, spec->nk, spec->lin_solver, max_block_smem(ctx->device),
+                                          w->threads ? w->threads[b] : kDefaultThreads);
     g.threads[b] = threads;
-    const int per_sm = resident_blocks(K, spec->nk, threads);
+    const int per_sm = resident_blocks(K, spec->nk, threads, spec->lin_solver);
     int full = (int)((float)(per_sm * ctx->sm_count) * rest);
     if (full < 1) full = 1;
     if (w->blocks_per_sm && w->blocks_per_sm[b] > 0 && w->blocks_per_sm[b] < per_sm)

@@ -95,6 +95,7 @@ inline Params make_params(const cbc_spec& s) {
   p.dense_mode = s.dense_mode;
   p.nk = s.nk;
   p.ac = s.ac;
+  p.lin = s.lin_solver;
   return p;
 }
 
@@ -110,6 +111,8 @@ inline int32_t check_spec(cbc_context* ctx, const cbc_spec* s) {
   if (s->ndo < 0) return fail(ctx, CBC_E_INVALID, "ndo must be >= 0");
   if (s->dense_mode < 0 || s->dense_mode > 1) return fail(ctx, CBC_E_INVALID, "dense_mode must be 0 or 1");
   if (s->lin_max_iter < 0) return fail(ctx, CBC_E_INVALID, "lin_max_iter must be >= 0");
+  if (s->lin_solver != CBC_LIN_RICHARDSON && s->lin_solver != CBC_LIN_LU)
+    return fail(ctx, CBC_E_INVALID, "lin_solver = %d: expected 0 (Richardson) or 1 (direct)", s->lin_solver);
   if (!(s->min_step > 0.0) || !(s->max_step >= s->min_step))
     return fail(ctx, CBC_E_INVALID, "need 0 < min_step <= max_step");
   if (!(s->atol > 0.0) || !(s->rtol >= 0.0)) return fail(ctx, CBC_E_INVALID, "need atol > 0, rtol >= 0");
@@ -126,6 +129,18 @@ constexpr size_t kScheduleBytes = kHeadBytes + 2 * sizeof(long long);
 // once per device.  *out stays NULL for device ordinals beyond its table.
 cudaError_t noalloc_scratch_address(int device, void** out);
 
+// Threads per block for a kernel of K bubbles per system: `requested`, cut
+// to whole warps whose shared memory fits the device's per-block limit
+// (K = 32 with its partner coefficients or augmented rows in shared memory
+// needs ~67 KB per warp, so at most three warps per block).
+inline int block_threads_for(int K, int nk, int lin, size_t max_block_smem, int requested) {
+  const size_t per_warp = sizeof(double) * (size_t)smem_doubles_per_warp(K, nk, lin);
+  int warps = requested / 32;
+  if (per_warp > 0 && (size_t)warps * per_warp > max_block_smem) warps = (int)(max_block_smem / per_warp);
+  if (warps < 1) warps = 1;
+  return warps * 32;
+}
+
 // Smallest power-of-two instantiation that holds K bubbles per system.
 inline int kb_for(int K) {
   if (K <= 2) return 2;
@@ -141,6 +156,13 @@ inline int kb_for(int K) {
 // (K read at run time).
 template <int V>
 using IC = std::integral_constant<int, V>;
+
+// Calls f(IC<LIN>) for the implicit-coupling solver of a launch.
+template <class F>
+decltype(auto) dispatch_lin(int lin, F&& f) {
+  if (lin == LIN_LU) return f(IC<LIN_LU>{});
+  return f(IC<LIN_RICHARDSON>{});
+}
 
 template <class F>
 decltype(auto) dispatch_k(int K, F&& f) {

@@ -33,6 +33,7 @@
 #pragma once
 
 #include <stdint.h>
+#include <utility>
 #include "cbc_math.h"
 
 namespace cbc {
@@ -86,6 +87,7 @@ struct Params {
   int dense_mode;  // 0 reference schedule, 1 exact grid
   int nk;          // harmonics
   int ac;          // 0 CONST, 1 SW_N, 2 SW_A
+  int lin;         // implicit-coupling solver: LIN_RICHARDSON or LIN_LU
 };
 
 // Position of this lane inside its system group.
@@ -148,26 +150,49 @@ struct WarpSmem {
   double* ks;   // [6][4][32]  stage derivatives, lane-private columns
   double* xv;   // [2][32] double2 partner-state exchange records
   double* cm;   // [3][K-1][32] coupling coefficients of each lane's partners d = 1..K-1
+  double* mat;  // implicit-coupling matrix rows (see mat_doubles), lane-private columns
+  double* pv;   // [G][2K+1] pivot-row snapshot of each group (direct solve, K > 8)
 };
 
 constexpr int XV_DOUBLES = 4 * 32;
+
+// Linear solvers of the implicit coupling system.
+enum : int { LIN_RICHARDSON = 0, LIN_LU = 1 };
 
 // Harmonic-constant region rounded up to an even count, so that every later
 // region (and every warp's carve-up) stays 16-byte aligned for double2 access.
 __host__ __device__ inline int hc_doubles(int K, int nk) { return (HC_PER_K * nk * (32 / K) + 1) & ~1; }
 
-__host__ __device__ inline int smem_doubles_per_warp(int K, int nk) {
-  return hc_doubles(K, nk) + NUPS * 32 + 24 * 32 + XV_DOUBLES + 3 * (K - 1) * 32;
+// Matrix region per warp:
+//   Richardson, K <= 8: none (the partner coefficients live in registers);
+//   Richardson, K > 8:  the four partner-coefficient arrays [4][K-1][32]
+//                       (kept out of registers: local memory would spill to L2);
+//   direct, K <= 8:     staging of the four coefficient blocks by absolute
+//                       column, [4][K][32], read back into register rows;
+//   direct, K > 8:      the two augmented rows of every lane, [2][2K+1][32].
+__host__ __device__ inline int mat_doubles(int K, int lin) {
+  if (K <= 8) return lin == LIN_LU ? 4 * K * 32 : 0;
+  return lin == LIN_LU ? 2 * (2 * K + 1) * 32 : 4 * (K - 1) * 32;
+}
+__host__ __device__ inline int pv_doubles(int K, int lin) {
+  return (K > 8 && lin == LIN_LU) ? (((32 / K) * (2 * K + 1) + 1) & ~1) : 0;
 }
 
-__device__ __forceinline__ WarpSmem warp_smem(double* base, int K, int nk) {
+__host__ __device__ inline int smem_doubles_per_warp(int K, int nk, int lin = LIN_RICHARDSON) {
+  return hc_doubles(K, nk) + NUPS * 32 + 24 * 32 + XV_DOUBLES + 3 * (K - 1) * 32 + mat_doubles(K, lin) +
+         pv_doubles(K, lin);
+}
+
+__device__ __forceinline__ WarpSmem warp_smem(double* base, int K, int nk, int lin = LIN_RICHARDSON) {
   WarpSmem w;
-  double* p = base + (threadIdx.x >> 5) * smem_doubles_per_warp(K, nk);
+  double* p = base + (threadIdx.x >> 5) * smem_doubles_per_warp(K, nk, lin);
   w.hc = p;
   w.up = p + hc_doubles(K, nk);
   w.ks = w.up + NUPS * 32;
   w.xv = w.ks + 24 * 32;
   w.cm = w.xv + XV_DOUBLES;
+  w.mat = w.cm + 3 * (K - 1) * 32;
+  w.pv = w.mat + mat_doubles(K, lin);
   return w;
 }
 
@@ -318,7 +343,8 @@ __device__ __forceinline__ double group_sum_full(double v) {
 // Residual r = b - A v of the implicit coupling system for this lane's bubble,
 // A = I + off-diagonal partner blocks.  Partner distance d = 1..K-1 goes to
 // accumulation chain (d - 1) mod 4 (increasing d within a chain); the chains
-// are then combined by the open pairwise tree.
+// are then combined by the open pairwise tree.  Coefficients from registers
+// (K <= 8) or from the lane's shared-memory columns (K > 8).
 template <int KB>
 __device__ __forceinline__ void residual(const Geo& g, const double* Am, const double* Bm, const double* Cm,
                                          const double* Dm, double cpf0, double b0, double b1, double vr,
@@ -340,7 +366,217 @@ __device__ __forceinline__ void residual(const Geo& g, const double* Am, const d
   r1 = b1 - (st + vt);
 }
 
+// The same with the coefficients in shared memory: m[(q (K-1) + d - 1) 32]
+// for q = 0..3 (A, B, C, D), m pointing at this lane's column.
 template <int KB>
+__device__ __forceinline__ void residual_smem(const Geo& g, const double* m, double cpf0, double b0, double b1,
+                                              double vr, double vt, double& r0, double& r1) {
+  double ar[4] = {0.0, 0.0, 0.0, 0.0}, at[4] = {0.0, 0.0, 0.0, 0.0};
+  const int K1 = g.K - 1;
+#pragma unroll
+  for (int d = 1; d < KB; ++d)
+    if (d < g.K) {
+      const int src = partner_lane(g, d);
+      const double vrj = shfl(vr, src), vtj = shfl(vt, src);
+      const int c = (d - 1) & 3;
+      const double A = m[(0 * K1 + d - 1) * 32], B = m[(1 * K1 + d - 1) * 32];
+      const double C = m[(2 * K1 + d - 1) * 32], D = m[(3 * K1 + d - 1) * 32];
+      ar[c] = fma(A, vrj, fma(B, vtj, ar[c]));
+      at[c] = fma(C, vrj, fma(D, vtj, at[c]));
+    }
+  const int nc = g.K - 1 < 4 ? g.K - 1 : 4;
+  const double sr = tree_open(ar, nc);
+  const double st = tree_open(at, nc);
+  r0 = b0 - fma(sr, cpf0, vr);
+  r1 = b1 - (st + vt);
+}
+
+// ---- direct solve of the implicit coupling system (lin_solver = LU) --------
+// Unknowns x = (vr_0..vr_{K-1}, vt_0..vt_{K-1}); row R_i (index i) and row T_i
+// (index K + i) are held by lane i:
+//   R_i: x_i + cpf0_i sum_j (A_ij vr_j + B_ij vt_j) = b0_i
+//   T_i: x_{K+i} + sum_j (C_ij vr_j + D_ij vt_j)    = b1_i
+// Gauss-Jordan elimination with partial pivoting, column c = 0..2K-1:
+//   p   = the not-yet-pivot row with the largest |a[r][c]| (NaN ranks below
+//         every number, ties go to the smaller row index; a warp-shuffle
+//         argmax over the system's lanes);
+//   rp  = 1 / a[p][c];  pk[k] = a[p][k] for k = c+1..2K (k = 2K: right side);
+//   every row r: l = (r == p) ? 0 : a[r][c] * rp,  a[r][k] = fma(-l, pk[k], a[r][k]).
+// Pivot rows are eliminated too (Gauss-Jordan), so x_c = a[p_c][2K] * rp_c
+// with no triangular back-substitution pass.  ok = every pivot nonzero and
+// finite.  oracle/ckm1d_oracle.cpp (lu_solve) performs the same operations.
+constexpr int NO_ROW = 1 << 20;
+
+__device__ __forceinline__ double piv_key(double v, int r) {
+  return r >= NO_ROW ? -2.0 : (v != v ? -1.0 : fabs(v));
+}
+__device__ __forceinline__ bool piv_better(double va, int ra, double vb, int rb) {
+  const double ka = piv_key(va, ra), kb = piv_key(vb, rb);
+  return ka > kb || (ka == kb && ra < rb);
+}
+
+// Argmax of (value, row) over the group, the same total order in every lane.
+template <int KB>
+__device__ __forceinline__ void group_argmax(double& v, int& r, const Geo& g) {
+#pragma unroll
+  for (int w = 1; w < KB; w <<= 1) {
+    if (w < g.K) {
+      const int q = (g.li ^ w) & ~(w - 1);
+      const int src = g.base + (q < g.K ? q : g.li);
+      const double vo = shfl(v, src);
+      const int ro = __shfl_sync(FULL, r, src);
+      if (q < g.K && piv_better(vo, ro, v, r)) {
+        v = vo;
+        r = ro;
+      }
+    }
+  }
+}
+
+// Candidate row of this lane for column c: the better of its rows that are
+// not pivots yet.
+__device__ __forceinline__ void lane_candidate(double vR, double vT, bool pR, bool pT, int li, int K, double& v,
+                                               int& r) {
+  const int rR = pR ? NO_ROW : li, rT = pT ? NO_ROW : K + li;
+  const bool takeR = piv_better(vR, rR, vT, rT);
+  v = takeR ? vR : vT;
+  r = takeR ? rR : rT;
+}
+
+// Register rows, exact K <= 8 known at compile time (every index static: the
+// column steps are expanded by template recursion, so the rows never leave
+// registers).  The four coefficient blocks were staged by absolute column in
+// W.mat.
+struct LuTrack {
+  bool pR, pT;       // this lane's rows R / T already pivot rows
+  int srcR, srcT;    // pivot rows of columns li and K + li
+  double rpR, rpT;   // their reciprocal pivots
+  bool ok;
+};
+
+template <int KC, int C>
+__device__ __forceinline__ void lu_column(const Geo& g, double (&rR)[2 * KC], double (&rT)[2 * KC], double& hR,
+                                          double& hT, LuTrack& t) {
+  constexpr int K = KC, N = 2 * KC;
+  const int li = g.li;
+  double piv;
+  int p;
+  lane_candidate(rR[C], rT[C], t.pR, t.pT, li, K, piv, p);
+  group_argmax<(KC <= 2 ? 2 : (KC <= 4 ? 4 : 8))>(piv, p, g);
+  t.ok = t.ok && (piv != 0.0) && cbcm::isfinite_(piv);
+  const double rp = 1.0 / piv;
+  const bool ps = p >= K;
+  const int src = g.base + (ps ? p - K : p);
+  const bool meR = (p == li), meT = (p == K + li);
+  t.pR = t.pR || meR;
+  t.pT = t.pT || meT;
+  t.srcR = (C == li) ? p : t.srcR;
+  t.rpR = (C == li) ? rp : t.rpR;
+  t.srcT = (C == K + li) ? p : t.srcT;
+  t.rpT = (C == K + li) ? rp : t.rpT;
+  const double lR = meR ? 0.0 : rR[C] * rp;
+  const double lT = meT ? 0.0 : rT[C] * rp;
+#pragma unroll
+  for (int k = C + 1; k < N; ++k) {
+    const double pk = shfl(ps ? rT[k] : rR[k], src);
+    rR[k] = fma(-lR, pk, rR[k]);
+    rT[k] = fma(-lT, pk, rT[k]);
+  }
+  const double ph = shfl(ps ? hT : hR, src);
+  hR = fma(-lR, ph, hR);
+  hT = fma(-lT, ph, hT);
+}
+
+template <int KC, int... Cs>
+__device__ __forceinline__ void lu_columns(const Geo& g, double (&rR)[2 * KC], double (&rT)[2 * KC], double& hR,
+                                           double& hT, LuTrack& t, std::integer_sequence<int, Cs...>) {
+  (lu_column<KC, Cs>(g, rR, rT, hR, hT, t), ...);
+}
+
+template <int KC>
+__device__ __forceinline__ void lu_solve_reg(const Geo& g, const WarpSmem& W, double cpf0, double b0, double b1,
+                                             double& xr, double& xt, bool& ok) {
+  constexpr int K = KC, N = 2 * KC;
+  const int li = g.li;
+  const double* m = W.mat + g.lane;
+  double rR[N], rT[N];
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const bool dg = (j == li);
+    rR[j] = dg ? 1.0 : cpf0 * m[(0 * K + j) * 32];
+    rR[K + j] = dg ? 0.0 : cpf0 * m[(1 * K + j) * 32];
+    rT[j] = dg ? 0.0 : m[(2 * K + j) * 32];
+    rT[K + j] = dg ? 1.0 : m[(3 * K + j) * 32];
+  }
+  double hR = b0, hT = b1;
+  LuTrack t{false, false, 0, 0, 0.0, 0.0, true};
+  lu_columns<KC>(g, rR, rT, hR, hT, t, std::make_integer_sequence<int, N>{});
+  ok = t.ok;
+  // x_c = h[p_c] * rp_c; this lane needs columns li and K + li
+  const int oR = g.base + (t.srcR >= K ? t.srcR - K : t.srcR), oT = g.base + (t.srcT >= K ? t.srcT - K : t.srcT);
+  const double aR = shfl(hR, oR), aT = shfl(hT, oR);
+  const double cR = shfl(hR, oT), cT = shfl(hT, oT);
+  xr = (t.srcR >= K ? aT : aR) * t.rpR;
+  xt = (t.srcT >= K ? cT : cR) * t.rpT;
+}
+
+// Shared-memory rows for K > 8 (K read at run time): lane column k of row
+// R at W.mat[k 32 + lane], of row T at W.mat[(RS + k) 32 + lane], RS = 2K + 1,
+// right side at k = 2K.  The pivot row is first copied to the group's
+// snapshot W.pv, so every row (the pivot row included) is updated from its
+// values before the column, exactly as the register form reads them.
+template <int KB>
+__device__ __forceinline__ void lu_solve_smem(const Geo& g, const WarpSmem& W, double& xr, double& xt, bool& ok) {
+  const int K = g.K, N = 2 * K, RS = N + 1;
+  const int li = g.li;
+  double* mR = W.mat + g.lane;
+  double* mT = W.mat + RS * 32 + g.lane;
+  double* pv = W.pv + g.grp * RS;
+  bool pR = false, pT = false;
+  int srcR = 0, srcT = 0;
+  double rpR = 0.0, rpT = 0.0;
+  ok = true;
+#pragma unroll 1
+  for (int c = 0; c < N; ++c) {
+    __syncwarp();
+    const double vR = mR[c * 32], vT = mT[c * 32];
+    double piv;
+    int p;
+    lane_candidate(vR, vT, pR, pT, li, K, piv, p);
+    group_argmax<KB>(piv, p, g);
+    ok = ok && (piv != 0.0) && cbcm::isfinite_(piv);
+    const double rp = 1.0 / piv;
+    const bool meR = (p == li), meT = (p == K + li);
+    pR = pR || meR;
+    pT = pT || meT;
+    srcR = (c == li) ? p : srcR;
+    rpR = (c == li) ? rp : rpR;
+    srcT = (c == K + li) ? p : srcT;
+    rpT = (c == K + li) ? rp : rpT;
+    // snapshot of the pivot row (its owner copies it)
+    if (g.valid && (meR || meT)) {
+      const double* own = meR ? mR : mT;
+      for (int k = c + 1; k <= N; ++k) pv[k] = own[k * 32];
+    }
+    __syncwarp();
+    const double lR = meR ? 0.0 : vR * rp;
+    const double lT = meT ? 0.0 : vT * rp;
+#pragma unroll 4
+    for (int k = c + 1; k <= N; ++k) {
+      const double pk = pv[k];
+      mR[k * 32] = fma(-lR, pk, mR[k * 32]);
+      mT[k * 32] = fma(-lT, pk, mT[k * 32]);
+    }
+  }
+  __syncwarp();
+  // lanes outside every group read their own column (always in range)
+  const int oR = g.valid ? g.base + (srcR >= K ? srcR - K : srcR) : g.lane;
+  const int oT = g.valid ? g.base + (srcT >= K ? srcT - K : srcT) : g.lane;
+  xr = W.mat[(srcR >= K ? RS * 32 : 0) + N * 32 + oR] * rpR;
+  xt = W.mat[(srcT >= K ? RS * 32 : 0) + N * 32 + oT] * rpT;
+}
+
+template <int KB, int KC, int LIN>
 __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSmem& W, const MView& M,
                                     double sp0, double sp3, bool on, double t, const double y[4],
                                     double dy[4], bool& conv, int& iters) {
@@ -397,8 +633,16 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
   }
 
   // ---- explicit coupling + matrix of the implicit system over partners ----
+  // The partner coefficients A, B, C, D of the implicit system go to
+  // registers (Richardson, K <= 8), to the lane's shared-memory columns by
+  // partner distance (Richardson, K > 8) or by absolute partner column (the
+  // direct solve: its staging area for K <= 8, its augmented rows for K > 8).
+  constexpr bool REG = (KB <= 8) && (LIN == LIN_RICHARDSON);
   double g0 = 0.0, g1 = 0.0, tn = 0.0, tg2 = 0.0, tg3 = 0.0;
-  double Am[KB], Bm[KB], Cm[KB], Dm[KB];
+  double Am[REG ? KB : 1], Bm[REG ? KB : 1], Cm[REG ? KB : 1], Dm[REG ? KB : 1];
+  double* mcol = W.mat + g.lane;
+  const int K1 = K - 1;
+  const int RS = 2 * K + 1;
   // partner states through the exchange records
   double2* xv2 = reinterpret_cast<double2*>(W.xv);
   __syncwarp();
@@ -407,7 +651,12 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
   __syncwarp();
 #pragma unroll
   for (int d = 1; d < KB; ++d) {
-    Am[d] = 0.0; Bm[d] = 0.0; Cm[d] = 0.0; Dm[d] = 0.0;
+    if constexpr (REG) {
+      Am[d] = 0.0;
+      Bm[d] = 0.0;
+      Cm[d] = 0.0;
+      Dm[d] = 0.0;
+    }
     if (d < K) {
       const int src = partner_rec(g, d);
       // partner state; its coupling terms are recomputed exactly as the
@@ -443,10 +692,34 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
         tn = fma(m1, t2, tn);
         tg2 = fma(m1, t1, tg2);
         tg3 = fma(m2, t1, tg3);
-        Am[d] = (m0 * rd) * j02;
-        Bm[d] = ((0.5 * m0) * srd2) * j03;
-        Cm[d] = -((m1 * srd2) * j02);
-        Dm[d] = -((m1 * rd3) * j03);
+        const double a_ = (m0 * rd) * j02;
+        const double b_ = ((0.5 * m0) * srd2) * j03;
+        const double c_ = -((m1 * srd2) * j02);
+        const double d_ = -((m1 * rd3) * j03);
+        if constexpr (REG) {
+          Am[d] = a_;
+          Bm[d] = b_;
+          Cm[d] = c_;
+          Dm[d] = d_;
+        } else if constexpr (LIN == LIN_RICHARDSON) {
+          mcol[(0 * K1 + d - 1) * 32] = a_;
+          mcol[(1 * K1 + d - 1) * 32] = b_;
+          mcol[(2 * K1 + d - 1) * 32] = c_;
+          mcol[(3 * K1 + d - 1) * 32] = d_;
+        } else {
+          const int j = partner_lane(g, d) - g.base;   // absolute partner column
+          if constexpr (KB <= 8) {
+            mcol[(0 * K + j) * 32] = a_;
+            mcol[(1 * K + j) * 32] = b_;
+            mcol[(2 * K + j) * 32] = c_;
+            mcol[(3 * K + j) * 32] = d_;
+          } else {
+            mcol[j * 32] = a_;              // row R (scaled by cpf0 below)
+            mcol[(K + j) * 32] = b_;
+            mcol[(RS + j) * 32] = c_;       // row T
+            mcol[(RS + K + j) * 32] = d_;
+          }
+        }
       }
     }
   }
@@ -477,6 +750,38 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
   b0 = fma(g0, cpf0, fma(g1, cpf1, b0));
   b1 = b1 + fma(tg2, cpf2, fma(tg3, cpf3, tn));
 
+  if constexpr (LIN == LIN_LU) {
+    // ---- implicit coupling: direct solve (Gauss-Jordan, partial pivoting) ----
+    // (the exact K is a compile-time constant whenever K <= 8)
+    static_assert(KB > 8 || KC > 0, "the register form needs the exact K");
+    double xr, xt;
+    bool okd;
+    if constexpr (KB <= 8) {
+      lu_solve_reg<(KC > 0 ? KC : 1)>(g, W, cpf0, b0, b1, xr, xt, okd);
+    } else {
+      // finish the augmented rows: scale row R by cpf0, diagonal, right sides
+      for (int j = 0; j < K; ++j) {
+        if (j == li) continue;
+        mcol[j * 32] = cpf0 * mcol[j * 32];
+        mcol[(K + j) * 32] = cpf0 * mcol[(K + j) * 32];
+      }
+      mcol[li * 32] = 1.0;
+      mcol[(K + li) * 32] = 0.0;
+      mcol[(2 * K) * 32] = b0;
+      mcol[(RS + li) * 32] = 0.0;
+      mcol[(RS + K + li) * 32] = 1.0;
+      mcol[(RS + 2 * K) * 32] = b1;
+      lu_solve_smem<KB>(g, W, xr, xt, okd);
+    }
+    iters = 1;
+    conv = okd || !on;
+    dy[0] = x2;
+    dy[1] = x3;
+    dy[2] = xr;
+    dy[3] = xt;
+    return;
+  }
+
   // ---- implicit coupling: relaxed Richardson from v = b (ckm1d_def.py:303-404) ----
   const double bn = group_sum<KB>(fma(b0, b0, b1 * b1), g);
   const double rt = P.lin_rtol2 * bn;
@@ -493,7 +798,8 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
   iters = 0;
   const bool full_groups = (g.K == KB);
   double r0, r1;
-  residual<KB>(g, Am, Bm, Cm, Dm, cpf0, b0, b1, vr, vt, r0, r1);
+  if constexpr (REG) residual<KB>(g, Am, Bm, Cm, Dm, cpf0, b0, b1, vr, vt, r0, r1);
+  else residual_smem<KB>(g, mcol, cpf0, b0, b1, vr, vt, r0, r1);
   for (int it = 0; it < P.lin_max_iter; ++it) {
     if (__all_sync(FULL, found)) break;
     const double rr = fma(r0, r0, r1 * r1);
@@ -507,7 +813,8 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
     found = found | hit;
     vr = fma(P.omega, r0, vr);
     vt = fma(P.omega, r1, vt);
-    residual<KB>(g, Am, Bm, Cm, Dm, cpf0, b0, b1, vr, vt, r0, r1);
+    if constexpr (REG) residual<KB>(g, Am, Bm, Cm, Dm, cpf0, b0, b1, vr, vt, r0, r1);
+    else residual_smem<KB>(g, mcol, cpf0, b0, b1, vr, vt, r0, r1);
   }
   conv = found;
   if (found) {
@@ -568,7 +875,7 @@ __device__ __forceinline__ void stage_state(const double* ks, double h, const do
 // One adaptive Cash-Karp step for every active group of the warp
 // (stepper.py:362-677).  Returns true (per lane) if a dense sample must be
 // stored after this step; the caller writes it.
-template <int KB>
+template <int KB, int KC, int LIN>
 __device__ __forceinline__ bool step(const Geo& g, const Params& P, const WarpSmem& W, const MView& M,
                                      LaneState& S) {
   const bool on = S.active;
@@ -610,7 +917,7 @@ __device__ __forceinline__ bool step(const Geo& g, const Params& P, const WarpSm
     double kk[4];
     bool cv;
     int it;
-    rhs<KB>(g, P, W, M, S.sp0, S.sp3, on, ts, ys, kk, cv, it);
+    rhs<KB, KC, LIN>(g, P, W, M, S.sp0, S.sp3, on, ts, ys, kk, cv, it);
 #pragma unroll
     for (int c = 0; c < 4; ++c) ks[(st * 4 + c) * 32] = kk[c];
     if (on) {

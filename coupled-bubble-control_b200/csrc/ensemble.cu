@@ -85,14 +85,14 @@ __device__ __forceinline__ void ens_writeback(const EnsLayout& E, const Params& 
 
 // Persistent worker: warps claim systems of bucket [begin, end) of the work
 // list until it is empty.  All systems of a bucket have the same K (<= KB).
-template <int KB, int KC>
+template <int KB, int KC, int LIN>
 __global__ void __launch_bounds__(128, min_blocks_for(KB)) ensemble_kernel(EnsLayout E, Params P, const int* __restrict__ order,
                                                        int begin, int end, int K, int* head,
                                                        long long max_steps, int steps_total,
                                                        const long long* epoch, long long budget_ns) {
   extern __shared__ __align__(16) double smem[];
   const Geo g = make_geo(KC > 0 ? KC : K);
-  const WarpSmem W = warp_smem(smem, g.K, P.nk);
+  const WarpSmem W = warp_smem(smem, g.K, P.nk, LIN);
   const int lane = threadIdx.x & 31;
   const bool leader = g.valid && g.li == 0;
 
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(128, min_blocks_for(KB)) ensemble_kernel(EnsLa
       continue;
     }
     // ---- one Cash-Karp step for every active slot ----
-    const bool stq = step<KB>(g, P, W, M, S);
+    const bool stq = step<KB, KC, LIN>(g, P, W, M, S);
     if (stq) ens_store_dense<KB>(E, S, g, sys, boff, S.idx);
     after_store(S, P, stq);
     if (S.active && S.steps + step_base >= max_steps) {
@@ -203,9 +203,9 @@ size_t max_block_smem(int device) {
 // that blocks of different bucket kernels can share an SM: with per-kernel
 // carveouts an SM configured for one kernel takes no block of another until it
 // drains, which serialises the buckets.
-template <int KB, int KC>
+template <int KB, int KC, int LIN>
 cudaError_t configure_ensemble_kernel(size_t shmem) {
-  cudaError_t e = cudaFuncSetAttribute(ensemble_kernel<KB, KC>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  cudaError_t e = cudaFuncSetAttribute(ensemble_kernel<KB, KC, LIN>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        (int)cudaSharedmemCarveoutMaxShared);
   // the opt-in limit is raised to the device maximum (never lowered again), so
   // a launch captured earlier with a larger request stays valid
@@ -215,7 +215,7 @@ cudaError_t configure_ensemble_kernel(size_t shmem) {
     const size_t cap = max_block_smem(dev);
     if (e == cudaSuccess) {
       if (shmem > cap) return cudaErrorInvalidValue;
-      e = cudaFuncSetAttribute(ensemble_kernel<KB, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+      e = cudaFuncSetAttribute(ensemble_kernel<KB, KC, LIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
     }
   }
   return e;
@@ -233,24 +233,28 @@ cudaError_t launch_ensemble_bucket(const EnsLayout& E, const Params& P, const in
                                    const long long* epoch, long long budget_ns, int blocks, int threads,
                                    cudaStream_t stream, size_t smem_bytes) {
   return dispatch_k(K, [&](auto kb, auto kc) {
-    constexpr int KB = decltype(kb)::value, KC = decltype(kc)::value;
-    size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, P.nk) * (threads / 32);
-    if (smem_bytes > shmem) shmem = smem_bytes;
-    cudaError_t e = configure_ensemble_kernel<KB, KC>(shmem);
-    if (e != cudaSuccess) return e;
-    ensemble_kernel<KB, KC><<<blocks, threads, shmem, stream>>>(E, P, order, begin, end, K, head, max_steps,
-                                                                steps_total, epoch, budget_ns);
-    return cudaGetLastError();
+    return dispatch_lin(P.lin, [&](auto lin) {
+      constexpr int KB = decltype(kb)::value, KC = decltype(kc)::value, LIN = decltype(lin)::value;
+      size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, P.nk, LIN) * (threads / 32);
+      if (smem_bytes > shmem) shmem = smem_bytes;
+      cudaError_t e = configure_ensemble_kernel<KB, KC, LIN>(shmem);
+      if (e != cudaSuccess) return e;
+      ensemble_kernel<KB, KC, LIN><<<blocks, threads, shmem, stream>>>(E, P, order, begin, end, K, head,
+                                                                       max_steps, steps_total, epoch, budget_ns);
+      return cudaGetLastError();
+    });
   });
 }
 
-int resident_blocks(int K, int nk, int threads) {
-  const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, nk) * (threads / 32);
+int resident_blocks(int K, int nk, int threads, int lin) {
+  const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, nk, lin) * (threads / 32);
   int n = 0;
   const cudaError_t e = dispatch_k(K, [&](auto kb, auto kc) {
-    constexpr int KB = decltype(kb)::value, KC = decltype(kc)::value;
-    configure_ensemble_kernel<KB, KC>(shmem);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<KB, KC>, threads, shmem);
+    return dispatch_lin(lin, [&](auto li) {
+      constexpr int KB = decltype(kb)::value, KC = decltype(kc)::value, LIN = decltype(li)::value;
+      configure_ensemble_kernel<KB, KC, LIN>(shmem);
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<KB, KC, LIN>, threads, shmem);
+    });
   });
   return (e == cudaSuccess && n > 0) ? n : 1;
 }

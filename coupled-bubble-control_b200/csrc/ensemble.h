@@ -61,6 +61,6 @@ cudaError_t launch_ensemble_bucket(const EnsLayout& E, const Params& P, const in
 // Writes the device clock (%globaltimer, ns) to *epoch.
 cudaError_t launch_stamp(long long* epoch, cudaStream_t stream);
 size_t max_block_smem(int device);
-int resident_blocks(int K, int nk, int threads);
+int resident_blocks(int K, int nk, int threads, int lin = LIN_RICHARDSON);
 
 }  // namespace cbc

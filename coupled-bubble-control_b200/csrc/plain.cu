@@ -43,12 +43,12 @@ __device__ __forceinline__ void ref_store_dense(const RefLayout& L, const LaneSt
   for (int c = 0; c < 4; ++c) L.dense_state[((long long)slot * 4 + c) * NST + s * L.tile + g.li] = S.y[c];
 }
 
-template <int KB, int KC>
+template <int KB, int KC, int LIN>
 __global__ void __launch_bounds__(128, min_blocks_for(KB)) plain_kernel(RefLayout L, Params P, long long budget, int final_launch,
                                                     int* active_counter) {
   extern __shared__ __align__(16) double smem[];
   const Geo g = make_geo(KC > 0 ? KC : L.ups);
-  const WarpSmem W = warp_smem(smem, L.ups, P.nk);
+  const WarpSmem W = warp_smem(smem, L.ups, P.nk, LIN);
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long s = warp * g.G + g.grp;
   const bool have = g.valid && s < L.ns;
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(128, min_blocks_for(KB)) plain_kernel(RefLayou
 
   for (long long it = 0; it < budget; ++it) {
     if (!__any_sync(FULL, S.active)) break;
-    const bool st = step<KB>(g, P, W, M, S);
+    const bool st = step<KB, KC, LIN>(g, P, W, M, S);
     if (st) ref_store_dense<KB>(L, S, g, s, S.idx);
     after_store(S, P, st);
   }
@@ -130,27 +130,37 @@ __global__ void __launch_bounds__(128, min_blocks_for(KB)) plain_kernel(RefLayou
   }
 }
 
-template <int KB, int KC>
+template <int KB, int KC, int LIN>
 cudaError_t launch_plain(const RefLayout& L, const Params& P, long long budget, int final_launch, int* counter,
                          cudaStream_t stream) {
   const int G = 32 / L.ups;
   const long long warps = (L.ns + G - 1) / G;
-  const int threads = 128;
+  int dev = 0;
+  cudaError_t de = cudaGetDevice(&dev);
+  if (de != cudaSuccess) return de;
+  int cap = 0;
+  de = cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (de != cudaSuccess) return de;
+  const int threads = block_threads_for(L.ups, P.nk, LIN, (size_t)cap, 128);
   const long long blocks = (warps * 32 + threads - 1) / threads;
-  const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(L.ups, P.nk) * (threads / 32);
+  const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(L.ups, P.nk, LIN) * (threads / 32);
   if (shmem > 48 * 1024) {
     cudaError_t e =
-        cudaFuncSetAttribute(plain_kernel<KB, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+        cudaFuncSetAttribute(plain_kernel<KB, KC, LIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
     if (e != cudaSuccess) return e;
   }
-  plain_kernel<KB, KC><<<(unsigned)blocks, threads, shmem, stream>>>(L, P, budget, final_launch, counter);
+  plain_kernel<KB, KC, LIN><<<(unsigned)blocks, threads, shmem, stream>>>(L, P, budget, final_launch, counter);
   return cudaGetLastError();
 }
 
 cudaError_t launch_plain_any(const RefLayout& L, const Params& P, long long budget, int final_launch,
                              int* counter, cudaStream_t stream) {
   return dispatch_k(L.ups, [&](auto kb, auto kc) {
-    return launch_plain<decltype(kb)::value, decltype(kc)::value>(L, P, budget, final_launch, counter, stream);
+    return dispatch_lin(P.lin, [&](auto lin) {
+      return launch_plain<decltype(kb)::value, decltype(kc)::value, decltype(lin)::value>(L, P, budget,
+                                                                                         final_launch, counter,
+                                                                                         stream);
+    });
   });
 }
 

@@ -47,6 +47,19 @@ extern "C" {
                                  device->host check whether every system finished */
 #define CBC_LAUNCH_SINGLE 1   /* one launch with the whole step budget, no host sync */
 
+/* ---- implicit-coupling solvers (cbc_spec.lin_solver) ----
+ * CBC_LIN_RICHARDSON: relaxed Richardson iteration v <- v + w (b - A v) from
+ *   v = b, stopped on the residual norm (reference ckm1d_def.py:303-404); the
+ *   reference's own (and the default) behaviour.
+ * CBC_LIN_LU: direct solve of the 2K x 2K system by Gauss-Jordan elimination
+ *   with partial pivoting (pivot search and pivot-row broadcast by warp
+ *   shuffles inside a system's lanes); exact to rounding, never fails to
+ *   converge (a zero or non-finite pivot counts as a convergence failure).
+ *   No counterpart in the reference's GPU kernels; its CPU path offers
+ *   direct-type solvers (reference/CKM1D_reference.py:364-518). */
+#define CBC_LIN_RICHARDSON 0
+#define CBC_LIN_LU 1
+
 typedef struct cbc_context cbc_context;
 
 /* Model/execution/solver specification.  Mirrors ModelSpec, ExecutionSpec and
@@ -69,6 +82,10 @@ typedef struct cbc_spec {
   double lin_relaxation;              /* 2/3                         */
   double etol;                        /* event tolerance, 1e-5       */
   double col_threshold;               /* collision gap factor - 1, 0.1 */
+  int32_t lin_solver;   /* implicit coupling: CBC_LIN_RICHARDSON (0, the
+                           reference's relaxed Richardson iteration) or
+                           CBC_LIN_LU (1, direct solve)                     */
+  int32_t reserved;
 } cbc_spec;
 
 /* Device buffers in the reference layout (models/model.py:56-106,

@@ -59,6 +59,8 @@ typedef struct cbo_spec {
   double lin_atol, lin_rtol, lin_relaxation;
   double etol;
   double col_threshold;  // collision threshold (0.1 in the numba kernel)
+  int32_t lin_solver;    // 0 relaxed Richardson (the reference), 1 direct (Gauss-Jordan, partial pivoting)
+  int32_t reserved;
 } cbo_spec;
 
 }  // extern "C"
@@ -126,8 +128,48 @@ void prepare(System& s) {
 
 struct Spec {
   double atol, rtol, min_step, max_step, lin_atol2, lin_rtol2, omega, etol, col;
-  int lin_max_iter, ndo, dense_mode;
+  int lin_max_iter, ndo, dense_mode, lin_solver;
 };
+
+// Direct solve of the implicit coupling system (lin_solver = 1), the same
+// operations as the device code (csrc/ckm1d_core.cuh, lu_solve_reg /
+// lu_solve_smem).  Unknowns x = (vr_0..vr_{K-1}, vt_0..vt_{K-1}); a holds N =
+// 2K rows of N + 1 entries (the right side last).  Gauss-Jordan elimination
+// with partial pivoting: for column c the pivot is the not-yet-pivot row with
+// the largest |a[r][c]| (NaN below every number, ties to the smaller row),
+// rp = 1 / pivot, the pivot row's entries k > c are read before the column's
+// updates, and every row r gets l = (r == p) ? 0 : a[r][c] * rp and
+// a[r][k] = fma(-l, pivot_row[k], a[r][k]) for k = c+1..N.  Then
+// x_c = a[p_c][N] * rp_c.  Returns false if a pivot is zero or not finite.
+bool lu_solve(int K, std::vector<double>& a, double* x) {
+  const int N = 2 * K, RS = N + 1;
+  auto key = [](double v) { return v != v ? -1.0 : fabs(v); };
+  bool pivoted[2 * KMAX] = {};
+  int perm[2 * KMAX];
+  double rps[2 * KMAX];
+  double pk[2 * KMAX + 1];
+  bool ok = true;
+  for (int c = 0; c < N; ++c) {
+    int p = -1;
+    for (int r = 0; r < N; ++r) {
+      if (pivoted[r]) continue;
+      if (p < 0 || key(a[(size_t)r * RS + c]) > key(a[(size_t)p * RS + c])) p = r;
+    }
+    const double piv = a[(size_t)p * RS + c];
+    ok = ok && (piv != 0.0) && cbcm::isfinite_(piv);
+    const double rp = 1.0 / piv;
+    pivoted[p] = true;
+    perm[c] = p;
+    rps[c] = rp;
+    for (int k = c + 1; k <= N; ++k) pk[k] = a[(size_t)p * RS + k];
+    for (int r = 0; r < N; ++r) {
+      const double l = (r == p) ? 0.0 : a[(size_t)r * RS + c] * rp;
+      for (int k = c + 1; k <= N; ++k) a[(size_t)r * RS + k] = fma(-l, pk[k], a[(size_t)r * RS + k]);
+    }
+  }
+  for (int c = 0; c < N; ++c) x[c] = a[(size_t)perm[c] * RS + N] * rps[c];
+  return ok;
+}
 
 // Pairwise-tree sum over the next power of two (zero padded):
 // ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + ...).
@@ -263,6 +305,42 @@ void rhs(const System& s, const Spec& sp, double t, const double (*y)[4], double
     }
     b0[i] = fma(g0, cpf0[i], fma(g1, cpf1[i], b0[i]));
     b1[i] = b1[i] + fma(tg2, cpf2[i], fma(tg3, cpf3[i], tn));
+  }
+
+  if (sp.lin_solver == 1) {
+    // direct solve: rows R_i (x_i + cpf0_i sum_j (A_ij vr_j + B_ij vt_j) = b0_i)
+    // and T_i (x_{K+i} + sum_j (C_ij vr_j + D_ij vt_j) = b1_i)
+    const int N = 2 * K, RS = N + 1;
+    static thread_local std::vector<double> a;
+    a.assign((size_t)N * RS, 0.0);
+    for (int i = 0; i < K; ++i) {
+      double* rR = &a[(size_t)i * RS];
+      double* rT = &a[(size_t)(K + i) * RS];
+      for (int j = 0; j < K; ++j) {
+        if (j == i) {
+          rR[j] = 1.0;
+          rR[K + j] = 0.0;
+          rT[j] = 0.0;
+          rT[K + j] = 1.0;
+        } else {
+          rR[j] = cpf0[i] * Am[(size_t)i * K + j];
+          rR[K + j] = cpf0[i] * Bm[(size_t)i * K + j];
+          rT[j] = Cm[(size_t)i * K + j];
+          rT[K + j] = Dm[(size_t)i * K + j];
+        }
+      }
+      rR[N] = b0[i];
+      rT[N] = b1[i];
+    }
+    double x[2 * KMAX];
+    const bool ok = lu_solve(K, a, x);
+    cnt.lin_iters += 1;
+    if (ok) cnt.conv_ok += 1; else cnt.conv_fail += 1;
+    for (int i = 0; i < K; ++i) {
+      dy[i][2] = x[i];
+      dy[i][3] = x[K + i];
+    }
+    return;
   }
 
   // implicit coupling: relaxed Richardson from v = b (ckm1d_def.py:303-404);
@@ -584,6 +662,7 @@ Spec make_spec(const cbo_spec* c) {
   s.lin_max_iter = c->lin_max_iter;
   s.ndo = c->ndo;
   s.dense_mode = c->dense_mode;
+  s.lin_solver = c->lin_solver;
   return s;
 }
 
@@ -607,7 +686,7 @@ int cbo_solve_ref_layout(const cbo_spec* spec, double* actual_time, const double
                          int32_t* rejected_steps, int32_t* conv_success, int32_t* conv_failures,
                          int64_t* lin_iters, int64_t budget, int32_t nthreads) {
   if (!spec || spec->ups < 1 || spec->ups > KMAX || spec->nk < 1 || spec->nk > NKMAX || spec->ns < 1 ||
-      spec->tile < spec->ups)
+      spec->tile < spec->ups || spec->lin_solver < 0 || spec->lin_solver > 1)
     return -1;
   const Spec sp = make_spec(spec);
   const int NS = spec->ns, K = spec->ups, T = spec->tile, NK = spec->nk, NDO = spec->ndo;
@@ -662,6 +741,17 @@ int cbo_solve_ref_layout(const cbo_spec* spec, double* actual_time, const double
   };
   run_parallel(worker, nthreads);
   return 0;
+}
+
+// The direct solver alone, for its unit tests: a holds the 2K x (2K + 1)
+// augmented matrix row-major (overwritten), x receives the 2K unknowns.
+// Returns 1 if every pivot was nonzero and finite, 0 if not, -1 on bad K.
+int cbo_lu_solve(int32_t K, double* a, double* x) {
+  if (K < 1 || K > KMAX) return -1;
+  std::vector<double> v(a, a + (size_t)2 * K * (2 * K + 1));
+  const bool ok = lu_solve(K, v, x);
+  std::copy(v.begin(), v.end(), a);
+  return ok ? 1 : 0;
 }
 
 // Elementary-function evaluator used by the unit tests of cbc_math.h.

@@ -16,6 +16,7 @@ _AC = {"CONST": 0, "SW_N": 1, "SW_A": 2}
 # "reference_defect" (oracle only): the reference's dense output as it is,
 # with its slot overwrite, for pinning against the reference's own samples
 _DENSE = {"reference": 0, "grid": 1, "reference_defect": 2}
+_LIN = {"richardson": 0, "lu": 1}
 
 
 class cbo_spec(ctypes.Structure):
@@ -25,7 +26,8 @@ class cbo_spec(ctypes.Structure):
                 ("atol", ctypes.c_double), ("rtol", ctypes.c_double), ("min_step", ctypes.c_double),
                 ("max_step", ctypes.c_double), ("lin_atol", ctypes.c_double),
                 ("lin_rtol", ctypes.c_double), ("lin_relaxation", ctypes.c_double),
-                ("etol", ctypes.c_double), ("col_threshold", ctypes.c_double)]
+                ("etol", ctypes.c_double), ("col_threshold", ctypes.c_double),
+                ("lin_solver", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 def _cpu_has_fma() -> bool:
@@ -58,6 +60,8 @@ def lib():
     L.cbo_solve_ref_layout.restype = ctypes.c_int
     L.cbo_math_eval.argtypes = [ctypes.c_int, ctypes.c_int64, P, P, P]
     L.cbo_math_eval.restype = None
+    L.cbo_lu_solve.argtypes = [ctypes.c_int32, P, P]
+    L.cbo_lu_solve.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -67,7 +71,7 @@ def make_spec(ns, ups, tile, ndo, nk, ac, solver_spec) -> cbo_spec:
     return cbo_spec(ns, ups, tile, ndo, nk, _AC[ac] if isinstance(ac, str) else int(ac),
                     _DENSE[getattr(s, "dense_mode", "reference")], int(s.lin_max_iter), s.atol, s.rtol,
                     s.min_step, s.max_step, s.lin_atol, s.lin_rtol, s.lin_relaxation, s.etol,
-                    getattr(s, "col_threshold", 0.1))
+                    getattr(s, "col_threshold", 0.1), _LIN[getattr(s, "lin_solver", "richardson")], 0)
 
 
 def _p(a: Optional[np.ndarray]):
@@ -127,3 +131,16 @@ def math_eval(kind: int, x: np.ndarray, y: Optional[np.ndarray] = None) -> np.nd
     out = np.empty_like(x)
     lib().cbo_math_eval(kind, x.size, x.ctypes.data, yy.ctypes.data, out.ctypes.data)
     return out
+
+
+def lu_solve(a: np.ndarray):
+    """The oracle's direct coupling solve on one augmented 2K x (2K+1) matrix:
+    (x, ok, eliminated matrix)."""
+    a = np.array(a, dtype=np.float64, order="C", copy=True)
+    n = a.shape[0]
+    assert n % 2 == 0 and a.shape == (n, n + 1)
+    x = np.zeros(n)
+    rc = lib().cbo_lu_solve(n // 2, a.ctypes.data, x.ctypes.data)
+    if rc < 0:
+        raise ValueError("bad K")
+    return x, bool(rc), a

@@ -12,8 +12,9 @@ against in ``oracle_configs.npz``:
   output is 8.5 MB, so the fixture holds a SHA-256 digest of every output
   buffer (reference layout, NaNs canonicalised) plus the end state and the
   counters in full for diagnosis.
-* ``mixed_k_2048``: 2,048 systems drawn from the 65,536-system mixed-K
-  ensemble (seed 1), stratified by K in proportion to its weights and, inside
+* ``mixed_k_2048``: 2,049 systems (2,048 split over K by its weights, each
+  count rounded) drawn from the 65,536-system mixed-K ensemble (seed 1),
+  stratified by K in proportion to its weights and, inside
   each K, evenly over the sorted spans, so spans run the whole 5-50 period
   range.  End state, times, step sizes, event values, statuses and counters
   are stored in full (ragged layout).

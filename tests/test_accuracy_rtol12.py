@@ -17,6 +17,19 @@ complete at both tolerances.  Observed maxima:
 (medians 3e-12 .. 1e-10; the maxima come from the collapse phase, where
 dR/dt changes by orders of magnitude within a few steps).  The bounds below
 guard against regressions with a margin.
+
+The direct coupling solve (lin_solver = "lu") at rtol = atol = 1e-9 against
+the tight direct-solve solution, same cases:
+
+  plain study:  R 3.4e-7  x 1.5e-10  U 7.4e-6  V 1.2e-6
+  mixed-K:      R <= 3.1e-8  x <= 2.0e-10  U <= 4.2e-6  V <= 6.3e-9
+  vec-env like: R 1.0e-7  x 1.2e-8   U 1.5e-7  V 1.8e-7
+  served like:  R 1.5e-9  x 3.9e-12  U 6.6e-8  V 1.8e-11
+  large-K:      R 6.3e-10 x 2.4e-14  U 8.7e-7  V 1.2e-9
+
+-- as accurate as the Richardson path or more (the iteration's 1e-9 residual
+is one more error source), and the tight Richardson and tight direct
+solutions agree to the digits above.
 """
 import copy
 
@@ -31,9 +44,9 @@ FLOOR = np.array([1.0, 1e-3, 1e-2, 1e-3])     # R, x, dR/dt, dx/dt
 BOUND = np.array([1e-5, 1e-6, 1e-4, 1e-4])
 
 
-def _run(scene, rtol, ndo):
+def _run(scene, rtol, ndo, lin="richardson"):
     spec_s = SolverSpec(rtol=rtol, atol=rtol, lin_rtol=min(1e-9, rtol), lin_atol=min(1e-9, rtol),
-                        dense_mode="grid")
+                        dense_mode="grid", lin_solver=lin)
     m = scenes.build_model(scene, solver_spec=spec_s, ndo=ndo)
     buf = copy.deepcopy(oracle.model_buffers(m))
     es, ms = m._execution_spec, m._model_spec
@@ -43,8 +56,8 @@ def _run(scene, rtol, ndo):
     return buf
 
 
-def _max_errors(scene, ndo):
-    a, b = _run(scene, 1e-9, ndo), _run(scene, 1e-12, ndo)
+def _max_errors(scene, ndo, lin="richardson"):
+    a, b = _run(scene, 1e-9, ndo, lin), _run(scene, 1e-12, ndo, lin)
     K = int(scene.K[0])
     ok = (a["status_flags"] == 1) & (b["status_flags"] == 1)
     assert np.any(ok)
@@ -74,4 +87,10 @@ def _cases():
 @pytest.mark.parametrize("name,scene,ndo", list(_cases()), ids=lambda v: v if isinstance(v, str) else "")
 def test_error_against_tight_tolerance(name, scene, ndo):
     e = _max_errors(scene, ndo)
+    assert np.all(e <= BOUND), f"{name}: max rel err (R, x, U, V) = {e}"
+
+
+@pytest.mark.parametrize("name,scene,ndo", list(_cases()), ids=lambda v: v if isinstance(v, str) else "")
+def test_direct_solve_error_against_tight_tolerance(name, scene, ndo):
+    e = _max_errors(scene, ndo, lin="lu")
     assert np.all(e <= BOUND), f"{name}: max rel err (R, x, U, V) = {e}"
