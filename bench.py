@@ -40,16 +40,28 @@ UNIT = "system-periods/s"
 MAX_STEPS = 1_000_000
 
 
-def flop_count(K, steps, lin_iters):
+def lu_flops(K):
+    """Flops of one direct solve (Gauss-Jordan with partial pivoting) of the
+    N = 2K coupling system: N^2 (N + 1) multiply-adds (fma = 2) over every row
+    and column, N^2 multipliers, N reciprocals, N products for x, and the
+    2K(K - 1) cpf0 scalings of the matrix rows."""
+    K = np.asarray(K, dtype=np.float64)
+    N = 2.0 * K
+    return N * N * (N + 1.0) + N * N + 2.0 * N + 2.0 * K * (K - 1.0)
+
+
+def flop_count(K, steps, lin_iters, lin_solver="richardson"):
     """Algorithmic FP64 flops (add/mul = 1, fma = 2, div/sqrt/pow/sin/cos = 1):
     per step 6 RHS of 130K + 35K^2 (uncoupled RHS + explicit coupling) plus
     240K + 10 (stages, error norm, controller), plus 20K^2 + 12K per
-    Richardson sweep of the implicit coupling."""
+    Richardson sweep of the implicit coupling, or lu_flops(K) per direct
+    solve (lin_iters counts sweeps, or solves)."""
     K = np.asarray(K, dtype=np.float64)
     steps = np.asarray(steps, dtype=np.float64)
     lin = np.asarray(lin_iters, dtype=np.float64)
     per_step = 6.0 * (130.0 * K + 35.0 * K ** 2) + 240.0 * K + 10.0
-    return float(np.sum(steps * per_step + lin * (20.0 * K ** 2 + 12.0 * K)))
+    per_lin = lu_flops(K) if lin_solver == "lu" else 20.0 * K ** 2 + 12.0 * K
+    return float(np.sum(steps * per_step + lin * per_lin))
 
 
 class ClockSampler:
@@ -232,7 +244,7 @@ def batched_once(scene, dev_index: int, schedule: str) -> float:
     return adv / dt
 
 
-def plain_per_k(scene, dev):
+def plain_per_k(scene, dev, solver_spec=None):
     """The reference execution model on the same systems: one reference-layout
     solve per K (cbc_solve, relaunch every 2048 steps with a host check)."""
     import torch
@@ -241,7 +253,7 @@ def plain_per_k(scene, dev):
     adv = 0.0
     for k in np.unique(scene.K):
         sel = np.nonzero(scene.K == k)[0]
-        m = scenes.build_model(scenes.subset(scene, sel), ndo=0)
+        m = scenes.build_model(scenes.subset(scene, sel), ndo=0, solver_spec=solver_spec)
         m._ensure_buffers()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -250,6 +262,80 @@ def plain_per_k(scene, dev):
         total += time.perf_counter() - t0
         adv += float(m.runtime.device_buffers.state.actual_time.sum().item())
     return adv / total, total
+
+
+def alone_latency(scene, dev_index: int, lin_solver: str, attempts: int = 3000):
+    """Per-attempt latency (us) of single systems running alone (one warp on
+    an otherwise idle GPU): for K = 2, 4 and 8, the longest-span system of
+    that K in the workload, `attempts` step attempts from its initial state."""
+    import torch
+    from cbc_b200 import scenes
+    from cbc_b200.ensemble import Ensemble
+    from cbc_b200.models import SolverSpec
+    out = {}
+    for k in (2, 4, 8):
+        sel = np.nonzero(scene.K == k)[0]
+        if sel.size == 0:
+            continue
+        s = int(sel[np.argmax(scene.t_end[sel])])
+        ens = Ensemble.from_scene(scenes.subset(scene, [s]), solver_spec=SolverSpec(lin_solver=lin_solver),
+                                  device=dev_index).to_device()
+        ens.solve(50)                      # load the kernel
+        ens.reset_device()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ens.solve(attempts)
+        b.record()
+        torch.cuda.synchronize()
+        n = int((ens.dev["steps"] + ens.dev["rejected"]).sum().item())
+        out[f"K{k}_us_per_attempt"] = a.elapsed_time(b) * 1e3 / max(n, 1)
+    return out
+
+
+def lu_arm(scene, dev_index: int, schedule: str, flush, max_steps: int = MAX_STEPS, plain: bool = True,
+           tune: bool = True):
+    """The same workload with the direct coupling solve (lin_solver = "lu"):
+    one untimed and one timed batched solve (L2 flushed before), its status
+    counts and roofline numerator, and optionally the plain per-K path."""
+    import torch
+    from cbc_b200.ensemble import Ensemble
+    from cbc_b200.models import SolverSpec
+    spec = SolverSpec(lin_solver="lu")
+    ens = Ensemble.from_scene(scene, solver_spec=spec, device=dev_index).to_device()
+    tune_info = None
+    if tune:
+        from cbc_b200.autotune import Autotuner
+        tuner = Autotuner(dev_index)
+        tuner.tune(ens)
+        tune_info = tuner.summary()
+    plan = make_plan(ens, schedule, max_steps)
+    pristine = {k: v.clone() for k, v in ens.dev.items()}
+    ms = None
+    for i in range(2):
+        for k in ("state", "t", "h", "event", "status", "steps", "rejected", "conv_ok", "conv_fail", "lin_iters"):
+            ens.dev[k].copy_(pristine[k])
+        flush.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        plan.launch()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+    plan.close()
+    res = ens.to_host()
+    adv = float(np.sum(res["t"] - ens.host["t"]))
+    flops = flop_count(res["K"], res["steps"], res["lin_iters"], "lu")
+    out = {"value": adv / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+           "advanced_system_periods_per_step": adv,
+           "status_counts": {int(k): int(v) for k, v in zip(*np.unique(res["status"], return_counts=True))},
+           "steps_per_solve": int(np.sum(res["steps"])), "algorithmic_gflop_per_step": flops / 1e9,
+           "achieved_tflops": flops / (ms * 1e-3) / 1e12, "autotune": tune_info}
+    if plain:
+        pv, ptime = plain_per_k(scene, None, spec)
+        out["plain"] = {"value": pv, "unit": UNIT, "seconds": ptime}
+        out["batched_vs_plain"] = out["value"] / pv
+    return out
 
 
 def env_step_latency(dev_index: int, n_steps: int = 128, warmup: int = 3):
@@ -298,6 +384,12 @@ def run_b200(args):
     scene = scenes.mixed_k(ns=args.ns, seed=rank_seed(rank))
     ens = Ensemble.from_scene(scene, device=local)
     ens.to_device()
+    tune_info = None
+    if args.tune:
+        from cbc_b200.autotune import Autotuner
+        tuner = Autotuner(local)
+        tuner.tune(ens)
+        tune_info = tuner.summary()
     plan = make_plan(ens, args.schedule, args.max_steps)
     nbuckets = int(np.unique(scene.K).size)
     # pristine device copy of the initial state for the per-step reset
@@ -372,6 +464,11 @@ def run_b200(args):
     if args.env and rank == 0:
         env_lat = env_step_latency(local)
 
+    lu = None
+    if args.lu and rank == 0:
+        lu = lu_arm(scene, local, args.schedule, flush, args.max_steps, plain=args.plain, tune=args.tune)
+        lu["alone_latency"] = alone_latency(scene, local, "lu")
+
     plain = None
     if args.plain and rank == 0:
         from cbc_b200 import scenes as _sc
@@ -394,7 +491,7 @@ def run_b200(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_all / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(args, world),
+            "config": {**workload_config(args, world), "autotune": tune_info},
             "work": {"advanced_system_periods_per_step": adv, "nominal_system_periods": float(np.sum(scene.t_end)),
                      "status_counts": status, "steps_per_solve": int(np.sum(res["steps"])),
                      "richardson_sweeps_per_rhs": float(np.sum(res["lin_iters"]) / max(1, 6 * np.sum(res["steps"]))),
@@ -413,6 +510,10 @@ def run_b200(args):
             line["e2e"] = e2e
         if env_lat:
             line["env_step_latency"] = env_lat
+        line["alone_latency"] = alone_latency(scene, local, "richardson")
+        if lu:
+            lu["roofline_frac"] = lu["achieved_tflops"] / peak
+            line["lin_solver_lu"] = lu
         if world == 1 and args.cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(scene)
         print(json.dumps(line), flush=True)
@@ -433,6 +534,10 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-env", dest="env", action="store_false")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="skip the autotuner (default launch shape for every K)")
+    ap.add_argument("--no-lu", dest="lu", action="store_false",
+                    help="skip the direct coupling-solve (lin_solver=lu) arm on the same workload")
     ap.add_argument("--plain-ns", type=int, default=0,
                     help="systems used for the batched-vs-plain ratio (0: the whole ensemble)")
     ap.add_argument("--e2e-steps", type=int, default=1)

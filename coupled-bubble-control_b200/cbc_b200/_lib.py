@@ -59,7 +59,7 @@ class cbc_ensemble(ctypes.Structure):
 class cbc_work(ctypes.Structure):
     _fields_ = [("order", P), ("nbuckets", i32), ("bucket_K", P), ("bucket_begin", P), ("threads", P),
                 ("blocks_per_sm", P), ("share", P), ("exclusive", P), ("budget_ns", i64),
-                ("steps_total", i32), ("reserved", i32)]
+                ("steps_total", i32), ("reserved", i32), ("slots", P), ("min_blocks", P)]
 
 
 class cbc_env_io(ctypes.Structure):

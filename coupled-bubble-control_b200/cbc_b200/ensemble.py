@@ -35,6 +35,8 @@ class WorkList:
     blocks_per_sm: Optional[np.ndarray] = None
     share: Optional[np.ndarray] = None   # (nb,) float32 fraction of the GPU per bucket at the start
     exclusive: Optional[np.ndarray] = None   # (nb,) int32 SMs of a latency lane (0: ordinary bucket)
+    slots: Optional[np.ndarray] = None       # (nb,) int32 systems per warp (autotuner)
+    min_blocks: Optional[np.ndarray] = None  # (nb,) int32 register-budget variant 0 / 1 (autotuner)
 
 
 # Steady-state cost of one step attempt on a full B200 (ns), measured on
@@ -170,6 +172,9 @@ class Ensemble:
         self.nb = int(host["state"].shape[0])
         self.dev: Dict[str, object] = {}
         self._plans: List[object] = []
+        # per-K launch shape chosen by cbc_b200.autotune (K -> TuneConfig);
+        # applied to every work list that does not set its own
+        self.tuning: Dict[int, object] = {}
 
     # ---- construction ----
     @classmethod
@@ -291,10 +296,6 @@ class Ensemble:
         keep += [bk, bb]
         w.bucket_K = bk.ctypes.data
         w.bucket_begin = bb.ctypes.data
-        if wl.threads is not None:
-            th = np.ascontiguousarray(wl.threads, dtype=np.int32)
-            keep.append(th)
-            w.threads = th.ctypes.data
         if wl.blocks_per_sm is not None:
             bp = np.ascontiguousarray(wl.blocks_per_sm, dtype=np.int32)
             keep.append(bp)
@@ -307,9 +308,36 @@ class Ensemble:
             ex = np.ascontiguousarray(wl.exclusive, dtype=np.int32)
             keep.append(ex)
             w.exclusive = ex.ctypes.data
+        tuned = self._tuned_arrays(wl)
+        for name in ("threads", "slots", "min_blocks"):
+            arr = getattr(wl, name, None)
+            if arr is None:
+                arr = tuned.get(name)
+            if arr is not None:
+                a = np.ascontiguousarray(arr, dtype=np.int32)
+                keep.append(a)
+                setattr(w, name, a.ctypes.data)
         w.budget_ns = int(budget_ns)
         w.steps_total = 1 if steps_total else 0
         return w, keep
+
+    def _tuned_arrays(self, wl: WorkList) -> Dict[str, np.ndarray]:
+        """threads / slots / min_blocks per bucket from self.tuning (latency
+        lanes keep the defaults: whole warps, the full register budget)."""
+        if not self.tuning:
+            return {}
+        nb = int(wl.bucket_K.size)
+        th = np.full(nb, 128, np.int32)
+        sl = np.asarray([32 // int(k) for k in wl.bucket_K], np.int32)
+        mb = np.zeros(nb, np.int32)
+        for b, k in enumerate(wl.bucket_K):
+            cfg = self.tuning.get(int(k))
+            if cfg is None or (wl.exclusive is not None and wl.exclusive[b] > 0):
+                continue
+            th[b] = cfg.threads
+            sl[b] = cfg.slots if cfg.slots > 0 else 32 // int(k)
+            mb[b] = cfg.min_blocks if int(k) <= 8 else 0
+        return {"threads": th, "slots": sl, "min_blocks": mb}
 
     # ---- solving ----
     def solve(self, max_steps: int = 1_000_000, work: Optional[WorkList] = None, stream=None,

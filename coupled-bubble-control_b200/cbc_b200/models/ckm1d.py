@@ -75,58 +75,29 @@ class CKM1D(Model):
             print("Padding Applied" if R0.shape != (ns, tile) else "NO Padding Applied (already padded)")
         self._initialize_host_buffers()
 
-    # ---- parameter precompute (reference ckm1d.py:133-188) ----
+    # ---- parameter precompute (reference ckm1d.py:133-202) ----
     def build_parameters(self):
         unit_params = np.zeros(self.unit_param_shape, dtype=np.float64)
         system_params = np.zeros(self.system_param_shape, dtype=np.float64)
         coupling_matrices = np.zeros(self.coupling_matrix_shape, dtype=np.float64)
-        TWO_PI = 2.0 * np.pi
-        mp = self.mat_props
-        PV, RHO, ST, VIS, CL, P0, PE = mp.PV, mp.RHO, mp.ST, mp.VIS, mp.CL, mp.P0, mp.PE
-        UPS = self._execution_spec.ups
-        w_ref = TWO_PI * self._REF_FREQ
-        l_ref = CL / self._REF_FREQ
-        R0 = self._R0[:, :UPS]
-        # Keller--Miksis
-        unit_params[0, :, :UPS] = (2.0 * ST / R0 + P0 - PV) * (TWO_PI / R0 / w_ref) ** 2.0 / RHO
-        unit_params[1, :, :UPS] = (1.0 - 3.0 * PE) * (2 * ST / R0 + P0 - PV) * (2.0 * np.pi / R0 / w_ref) / CL / RHO
-        unit_params[2, :, :UPS] = (P0 - PV) * (2.0 * np.pi / R0 / w_ref) ** 2.0 / RHO
-        unit_params[3, :, :UPS] = (2.0 * ST / R0 / RHO) * (TWO_PI / R0 / w_ref) ** 2.0
-        unit_params[4, :, :UPS] = 4.0 * VIS / RHO / (R0 ** 2.0) * (2.0 * np.pi / w_ref)
-        unit_params[5, :, :UPS] = ((2.0 * np.pi / R0 / w_ref) ** 2.0) / RHO
-        unit_params[6, :, :UPS] = ((2.0 * np.pi / w_ref) ** 2.0) / CL / RHO / R0
-        unit_params[7, :, :UPS] = R0 * w_ref / (2 * np.pi) / CL
-        # translational motion
-        unit_params[8, :, :UPS] = (0.5 * l_ref / R0) ** 2
-        unit_params[9, :, :UPS] = TWO_PI / RHO / R0 / l_ref / (w_ref * R0) ** 2.0
-        unit_params[10, :, :UPS] = 2 * TWO_PI / 3 * R0 ** 3
-        unit_params[11, :, :UPS] = 6 * TWO_PI * VIS * R0
-        unit_params[12, :, :UPS] = R0 / l_ref
-        # shared
-        system_params[0] = 3.0 * PE
-        system_params[1] = 1.0 / w_ref
-        system_params[2] = l_ref / TWO_PI
-        system_params[3] = CL
-        system_params[4] = 1 / RHO / CL
-        # coupling matrices, row = source bubble j, last axis = receiving bubble i
-        l_ref_mx = np.full_like(R0, l_ref)
-        for row in range(UPS):
-            coupling_matrices[0, row, :, :UPS] = R0[:, row:row + 1] ** 3 / R0 ** 2 / l_ref
-            coupling_matrices[1, row, :, :UPS] = 3.0 * (R0[:, row:row + 1] / l_ref_mx) ** 3
-            coupling_matrices[2, row, :, :UPS] = (18 * VIS / RHO) * (TWO_PI / w_ref) * (R0[:, row:row + 1] / l_ref) ** 3 / (R0 ** 2)
-        idx = np.arange(UPS)
-        coupling_matrices[:, idx, :, idx] = 0.0   # no self coupling
+        ups = self._execution_spec.ups
+        c = precompute_constants(self.mat_props, self._REF_FREQ)
+        R0 = self._R0[:, :ups]
+        unit_params[:, :, :ups] = bubble_constants(R0, c)
+        system_params[:] = np.asarray(system_constants(c))[:, None]
+        # coupling_matrices[m, j, s, i]: source bubble j, receiving bubble i
+        cm = coupling_constants(R0, c)                       # (3, ns, j, i)
+        coupling_matrices[:, :ups, :, :ups] = np.transpose(cm, (0, 2, 1, 3))
         return unit_params, system_params, coupling_matrices
 
     def build_control_parameters(self):
         control_params = np.zeros(self.control_param_shape, dtype=np.float64)
-        TWO_PI = 2.0 * np.pi
-        CL = self.mat_props.CL
-        NC = self._model_spec.nk
-        control_params[0:NC, :] = self._PA
-        control_params[NC:2 * NC, :] = self._FREQ * TWO_PI
-        control_params[2 * NC:3 * NC, :] = self._PS
-        control_params[3 * NC:4 * NC, :] = TWO_PI * self._FREQ / CL
+        nk = self._model_spec.nk
+        c = precompute_constants(self.mat_props, self._REF_FREQ)
+        control_params[0:nk, :] = self._PA
+        control_params[nk:2 * nk, :] = self._FREQ * c["two_pi"]
+        control_params[2 * nk:3 * nk, :] = self._PS
+        control_params[3 * nk:4 * nk, :] = c["two_pi"] * self._FREQ / c["CL"]
         return control_params
 
     def build_default_initial_state(self):
@@ -143,3 +114,85 @@ class CKM1D(Model):
             kernel = load_kernel(self._model_spec, self._execution_spec, self._solver_spec)
             return partial(solver, kernel=kernel)
         raise NotImplementedError(f"backend {b!r} is not served by this package (use BackendName.B200)")
+
+
+# ---- the precompute as array formulas over the radii -----------------------
+# The same arithmetic as the reference's build_parameters
+# (models/ckm1d.py:133-188) and build_control_parameters (:190-202), written
+# as products and quotients of per-bubble arrays and scalar constants so that
+# the device precompute (csrc/admit.cu) can repeat it operation for operation.
+# The one deliberate difference: cubes are (x * x) * x instead of numpy's
+# x ** 3 (a libm pow call, which a GPU cannot reproduce bit for bit); the two
+# differ by at most an ulp.
+
+def precompute_constants(mp, ref_freq_hz: float) -> dict:
+    """Scalar constants of the precompute (Python floats, host-evaluated)."""
+    two_pi = 2.0 * np.pi
+    w_ref = two_pi * ref_freq_hz
+    l_ref = mp.CL / ref_freq_hz
+    return {
+        "two_pi": two_pi, "w_ref": w_ref, "l_ref": l_ref,
+        "RHO": mp.RHO, "CL": mp.CL, "P0": mp.P0, "PV": mp.PV, "PE": mp.PE, "ST": mp.ST, "VIS": mp.VIS,
+        "st2": 2.0 * mp.ST,                           # 2 sigma
+        "k1": 1.0 - 3.0 * mp.PE,                      # 1 - 3 gamma
+        "p0pv": mp.P0 - mp.PV,
+        "k4": 4.0 * mp.VIS / mp.RHO,
+        "tw": two_pi / w_ref,                         # 2 pi / omega_ref
+        "k6": ((two_pi / w_ref) ** 2.0) / mp.CL / mp.RHO,
+        "hl": 0.5 * l_ref,
+        "k9": two_pi / mp.RHO,
+        "k10": 2 * two_pi / 3,
+        "k11": 6 * two_pi * mp.VIS,
+        "km2": (18 * mp.VIS / mp.RHO) * (two_pi / w_ref),
+    }
+
+
+def bubble_constants(R0: np.ndarray, c: dict) -> np.ndarray:
+    """The 13 per-bubble constants (unit_params) of radii R0 (m), any shape:
+    result shape (13,) + R0.shape."""
+    R0 = np.asarray(R0, dtype=np.float64)
+    s = c["two_pi"] / R0 / c["w_ref"]
+    s2 = s * s
+    pe = c["st2"] / R0 + c["P0"] - c["PV"]
+    q = c["hl"] / R0
+    wr = c["w_ref"] * R0
+    out = np.empty((13,) + R0.shape)
+    # Keller--Miksis
+    out[0] = pe * s2 / c["RHO"]
+    out[1] = c["k1"] * pe * s / c["CL"] / c["RHO"]
+    out[2] = c["p0pv"] * s2 / c["RHO"]
+    out[3] = (c["st2"] / R0 / c["RHO"]) * s2
+    out[4] = c["k4"] / (R0 * R0) * c["tw"]
+    out[5] = s2 / c["RHO"]
+    out[6] = c["k6"] / R0
+    out[7] = R0 * c["w_ref"] / c["two_pi"] / c["CL"]
+    # translational motion
+    out[8] = q * q
+    out[9] = c["k9"] / R0 / c["l_ref"] / (wr * wr)
+    out[10] = c["k10"] * ((R0 * R0) * R0)
+    out[11] = c["k11"] * R0
+    out[12] = R0 / c["l_ref"]
+    return out
+
+
+def system_constants(c: dict):
+    """The 5 per-system constants (system_params)."""
+    return [3.0 * c["PE"], 1.0 / c["w_ref"], c["l_ref"] / c["two_pi"], c["CL"], 1 / c["RHO"] / c["CL"]]
+
+
+def coupling_constants(R0: np.ndarray, c: dict) -> np.ndarray:
+    """Coupling coefficients of systems with radii R0 (ns, K) in metres:
+    (3, ns, K, K) indexed [m, s, j, i] (source bubble j, receiving bubble i),
+    zero for j == i."""
+    R0 = np.asarray(R0, dtype=np.float64)
+    Rj = R0[:, :, None]                   # source
+    Ri = R0[:, None, :]                   # receiver
+    rl = Rj / c["l_ref"]
+    out = np.empty((3,) + Rj.shape[:2] + (R0.shape[1],))
+    out[0] = ((Rj * Rj) * Rj) / (Ri * Ri) / c["l_ref"]
+    out[1] = 3.0 * ((rl * rl) * rl)
+    out[2] = c["km2"] * ((rl * rl) * rl) / (Ri * Ri)
+    K = R0.shape[1]
+    idx = np.arange(K)
+    out[:, :, idx, idx] = 0.0             # no self coupling
+    return out

@@ -54,6 +54,10 @@ static int32_t check_ensemble(cbc_context* ctx, const cbc_spec* spec, const cbc_
       return fail(ctx, CBC_E_INVALID, "bucket %d: threads per block must be 32..128, a multiple of 32", b);
     if (w->exclusive && w->exclusive[b] < 0)
       return fail(ctx, CBC_E_INVALID, "bucket %d: exclusive must be >= 0", b);
+    if (w->slots && (w->slots[b] < 1 || w->slots[b] > 32 / K))
+      return fail(ctx, CBC_E_INVALID, "bucket %d: slots = %d, need 1..%d for K = %d", b, w->slots[b], 32 / K, K);
+    if (w->min_blocks && (w->min_blocks[b] < 0 || w->min_blocks[b] > 1))
+      return fail(ctx, CBC_E_INVALID, "bucket %d: min_blocks variant must be 0 or 1", b);
   }
   if (w->budget_ns < 0) return fail(ctx, CBC_E_INVALID, "budget_ns must be >= 0");
   if (w->steps_total != 0 && w->steps_total != 1) return fail(ctx, CBC_E_INVALID, "steps_total must be 0 or 1");
@@ -128,6 +132,7 @@ struct GridsT {
   V<int> first, second, threads;
   V<size_t> smem;      // dynamic shared memory request (0: what the kernel needs)
   V<char> exclusive;
+  V<int> slots, mb;    // systems per warp, register-budget variant
 };
 using Grids = GridsT<HeapVec>;
 
@@ -143,6 +148,12 @@ static G grid_sizes(cbc_context* ctx, const cbc_spec* spec, const cbc_work* w) {
   g.threads.assign(w->nbuckets, kDefaultThreads);
   g.smem.assign(w->nbuckets, 0);
   g.exclusive.assign(w->nbuckets, 0);
+  g.slots.assign(w->nbuckets, 32);
+  g.mb.assign(w->nbuckets, 0);
+  for (int b = 0; b < w->nbuckets; ++b) {
+    if (w->slots) g.slots[b] = w->slots[b];
+    if (w->min_blocks && w->bucket_K[b] <= 8) g.mb[b] = w->min_blocks[b];
+  }
   // latency lanes first: one block per SM each
   int excl_sms = 0;
   for (int b = 0; b < w->nbuckets; ++b) {
@@ -165,13 +176,14 @@ static G grid_sizes(cbc_context* ctx, const cbc_spec* spec, const cbc_work* w) {
     const int threads = block_threads_for(K, spec->nk, spec->lin_solver, max_block_smem(ctx->device),
                                           w->threads ? w->threads[b] : kDefaultThreads);
     g.threads[b] = threads;
-    const int per_sm = resident_blocks(K, spec->nk, threads, spec->lin_solver);
+    const int per_sm = resident_blocks(K, spec->nk, threads, spec->lin_solver, g.mb[b]);
     int full = (int)((float)(per_sm * ctx->sm_count) * rest);
     if (full < 1) full = 1;
     if (w->blocks_per_sm && w->blocks_per_sm[b] > 0 && w->blocks_per_sm[b] < per_sm)
       full = (int)((float)(w->blocks_per_sm[b] * ctx->sm_count) * rest);
     if (full < 1) full = 1;
-    const long long warps_needed = ((long long)(end - begin) + (32 / K) - 1) / (32 / K);
+    const int per_warp = (32 / K < g.slots[b]) ? 32 / K : g.slots[b];
+    const long long warps_needed = ((long long)(end - begin) + per_warp - 1) / per_warp;
     const long long blocks_needed = (warps_needed * 32 + threads - 1) / threads;
     if (full > blocks_needed) full = (int)blocks_needed;
     if (w->share) {
@@ -225,7 +237,7 @@ static int32_t enqueue(cbc_context* ctx, const cbc_spec* spec, const cbc_ensembl
       CBC_CUDA_TRY(ctx, cudaStreamWaitEvent(s, ctx->fork, 0));
       CBC_CUDA_TRY(ctx, launch_ensemble_bucket(E, P, w->order, begin, end, K, d_head + b, max_steps,
                                                w->steps_total, epoch, w->budget_ns, blocks, grids.threads[b], s,
-                                               grids.smem[b]));
+                                               grids.smem[b], grids.slots[b], grids.mb[b]));
       ++ctx->launches;
       CBC_CUDA_TRY(ctx, cudaEventRecord(ctx->join[slot], s));
       CBC_CUDA_TRY(ctx, cudaStreamWaitEvent(stream, ctx->join[slot], 0));

@@ -164,6 +164,13 @@ decltype(auto) dispatch_lin(int lin, F&& f) {
   return f(IC<LIN_RICHARDSON>{});
 }
 
+// Calls f(IC<MB>) for the register-budget variant of a batched launch.
+template <class F>
+decltype(auto) dispatch_mb(int mb, F&& f) {
+  if (mb == 1) return f(IC<1>{});
+  return f(IC<0>{});
+}
+
 template <class F>
 decltype(auto) dispatch_k(int K, F&& f) {
   switch (K) {

@@ -72,6 +72,12 @@ static __constant__ double kStageB[6][5] = {{0, 0, 0, 0, 0},
 // memory either way).
 __host__ __device__ constexpr int min_blocks_for(int KB) { return KB <= 2 ? 4 : (KB <= 4 ? 3 : (KB <= 8 ? 2 : 1)); }
 
+// Register-budget variant MB of the batched kernels: MB = 1 asks ptxas for one
+// more resident 128-thread block per SM (fewer registers per thread, possibly
+// spills; more warps to hide latency).  The autotuner measures which is
+// faster.  K > 8 kernels are limited by shared memory and have only MB = 0.
+__host__ __device__ constexpr int min_blocks_variant(int KB, int MB) { return min_blocks_for(KB) + (KB <= 8 ? MB : 0); }
+
 // Per-system status codes (stepper.py:27-33).
 enum : int {
   ST_ACTIVE = 0, ST_SUCCESS = 1, ST_EVENT = 2,
@@ -101,12 +107,14 @@ struct Geo {
   bool valid;  // lane belongs to a group
 };
 
-__device__ __forceinline__ Geo make_geo(int K) {
+// slots: systems a warp holds at most (fewer than 32 / K leaves lanes idle:
+// less intra-warp divergence for fewer systems in flight; a tuning knob).
+__device__ __forceinline__ Geo make_geo(int K, int slots = 32) {
   Geo g;
   const int lane = threadIdx.x & 31;
   g.lane = lane;
   g.K = K;
-  g.G = 32 / K;
+  g.G = 32 / K < slots ? 32 / K : slots;
   const int grp = lane / K;
   g.valid = grp < g.G;
   g.grp = g.valid ? grp : 0;

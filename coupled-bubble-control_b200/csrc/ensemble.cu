@@ -85,13 +85,13 @@ __device__ __forceinline__ void ens_writeback(const EnsLayout& E, const Params& 
 
 // Persistent worker: warps claim systems of bucket [begin, end) of the work
 // list until it is empty.  All systems of a bucket have the same K (<= KB).
-template <int KB, int KC, int LIN>
-__global__ void __launch_bounds__(128, min_blocks_for(KB)) ensemble_kernel(EnsLayout E, Params P, const int* __restrict__ order,
-                                                       int begin, int end, int K, int* head,
-                                                       long long max_steps, int steps_total,
-                                                       const long long* epoch, long long budget_ns) {
+template <int KB, int KC, int LIN, int MB>
+__global__ void __launch_bounds__(128, min_blocks_variant(KB, MB))
+    ensemble_kernel(EnsLayout E, Params P, const int* __restrict__ order, int begin, int end, int K, int* head,
+                    long long max_steps, int steps_total, const long long* epoch, long long budget_ns,
+                    int slots) {
   extern __shared__ __align__(16) double smem[];
-  const Geo g = make_geo(KC > 0 ? KC : K);
+  const Geo g = make_geo(KC > 0 ? KC : K, slots);
   const WarpSmem W = warp_smem(smem, g.K, P.nk, LIN);
   const int lane = threadIdx.x & 31;
   const bool leader = g.valid && g.li == 0;
@@ -203,9 +203,9 @@ size_t max_block_smem(int device) {
 // that blocks of different bucket kernels can share an SM: with per-kernel
 // carveouts an SM configured for one kernel takes no block of another until it
 // drains, which serialises the buckets.
-template <int KB, int KC, int LIN>
+template <int KB, int KC, int LIN, int MB>
 cudaError_t configure_ensemble_kernel(size_t shmem) {
-  cudaError_t e = cudaFuncSetAttribute(ensemble_kernel<KB, KC, LIN>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  cudaError_t e = cudaFuncSetAttribute(ensemble_kernel<KB, KC, LIN, MB>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        (int)cudaSharedmemCarveoutMaxShared);
   // the opt-in limit is raised to the device maximum (never lowered again), so
   // a launch captured earlier with a larger request stays valid
@@ -215,7 +215,7 @@ cudaError_t configure_ensemble_kernel(size_t shmem) {
     const size_t cap = max_block_smem(dev);
     if (e == cudaSuccess) {
       if (shmem > cap) return cudaErrorInvalidValue;
-      e = cudaFuncSetAttribute(ensemble_kernel<KB, KC, LIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+      e = cudaFuncSetAttribute(ensemble_kernel<KB, KC, LIN, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
     }
   }
   return e;
@@ -231,29 +231,35 @@ cudaError_t launch_stamp(long long* epoch, cudaStream_t stream) {
 cudaError_t launch_ensemble_bucket(const EnsLayout& E, const Params& P, const int* order, int begin, int end,
                                    int K, int* head, long long max_steps, int steps_total,
                                    const long long* epoch, long long budget_ns, int blocks, int threads,
-                                   cudaStream_t stream, size_t smem_bytes) {
+                                   cudaStream_t stream, size_t smem_bytes, int slots, int mb) {
   return dispatch_k(K, [&](auto kb, auto kc) {
     return dispatch_lin(P.lin, [&](auto lin) {
-      constexpr int KB = decltype(kb)::value, KC = decltype(kc)::value, LIN = decltype(lin)::value;
-      size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, P.nk, LIN) * (threads / 32);
-      if (smem_bytes > shmem) shmem = smem_bytes;
-      cudaError_t e = configure_ensemble_kernel<KB, KC, LIN>(shmem);
-      if (e != cudaSuccess) return e;
-      ensemble_kernel<KB, KC, LIN><<<blocks, threads, shmem, stream>>>(E, P, order, begin, end, K, head,
-                                                                       max_steps, steps_total, epoch, budget_ns);
-      return cudaGetLastError();
+      return dispatch_mb(decltype(kb)::value <= 8 ? mb : 0, [&](auto mbv) {
+        constexpr int KB = decltype(kb)::value, KC = decltype(kc)::value, LIN = decltype(lin)::value,
+                      MB = decltype(mbv)::value;
+        size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, P.nk, LIN) * (threads / 32);
+        if (smem_bytes > shmem) shmem = smem_bytes;
+        cudaError_t e = configure_ensemble_kernel<KB, KC, LIN, MB>(shmem);
+        if (e != cudaSuccess) return e;
+        ensemble_kernel<KB, KC, LIN, MB><<<blocks, threads, shmem, stream>>>(
+            E, P, order, begin, end, K, head, max_steps, steps_total, epoch, budget_ns, slots);
+        return cudaGetLastError();
+      });
     });
   });
 }
 
-int resident_blocks(int K, int nk, int threads, int lin) {
+int resident_blocks(int K, int nk, int threads, int lin, int mb) {
   const size_t shmem = sizeof(double) * (size_t)smem_doubles_per_warp(K, nk, lin) * (threads / 32);
   int n = 0;
   const cudaError_t e = dispatch_k(K, [&](auto kb, auto kc) {
     return dispatch_lin(lin, [&](auto li) {
-      constexpr int KB = decltype(kb)::value, KC = decltype(kc)::value, LIN = decltype(li)::value;
-      configure_ensemble_kernel<KB, KC, LIN>(shmem);
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<KB, KC, LIN>, threads, shmem);
+      return dispatch_mb(decltype(kb)::value <= 8 ? mb : 0, [&](auto mbv) {
+        constexpr int KB = decltype(kb)::value, KC = decltype(kc)::value, LIN = decltype(li)::value,
+                      MB = decltype(mbv)::value;
+        configure_ensemble_kernel<KB, KC, LIN, MB>(shmem);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<KB, KC, LIN, MB>, threads, shmem);
+      });
     });
   });
   return (e == cudaSuccess && n > 0) ? n : 1;

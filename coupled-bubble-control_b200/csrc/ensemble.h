@@ -57,10 +57,10 @@ __device__ __forceinline__ long long global_ns() {
 cudaError_t launch_ensemble_bucket(const EnsLayout& E, const Params& P, const int* order, int begin, int end,
                                    int K, int* head, long long max_steps, int steps_total,
                                    const long long* epoch, long long budget_ns, int blocks, int threads,
-                                   cudaStream_t stream, size_t smem_bytes = 0);
+                                   cudaStream_t stream, size_t smem_bytes = 0, int slots = 32, int mb = 0);
 // Writes the device clock (%globaltimer, ns) to *epoch.
 cudaError_t launch_stamp(long long* epoch, cudaStream_t stream);
 size_t max_block_smem(int device);
-int resident_blocks(int K, int nk, int threads, int lin = LIN_RICHARDSON);
+int resident_blocks(int K, int nk, int threads, int lin = LIN_RICHARDSON, int mb = 0);
 
 }  // namespace cbc

@@ -246,6 +246,15 @@ typedef struct cbc_work {
    * stops every system at exactly the step a single call would. */
   int32_t steps_total;
   int32_t reserved;
+  /* Tuning (host arrays, may be NULL; results never depend on them):
+   * slots[b] systems held per warp, 1..32/K (default 32/K: every lane
+   * busy; fewer lowers intra-warp divergence); min_blocks[b] the
+   * register-budget variant of the bucket's kernel, 0 (default) or 1 (one
+   * more resident block per SM asked of the compiler, fewer registers per
+   * thread; K <= 8 only, ignored above).  Chosen per K by the project's
+   * autotuner (cbc_b200/autotune.py) together with threads. */
+  const int32_t* slots;
+  const int32_t* min_blocks;
 } cbc_work;
 
 typedef struct cbc_plan cbc_plan;
