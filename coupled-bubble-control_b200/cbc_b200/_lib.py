@@ -67,6 +67,17 @@ class cbc_env_io(ctypes.Structure):
                 ("failed", P), ("K", i32), ("pad", i32), ("t_span", f64), ("h0", f64)]
 
 
+class cbc_precompute_consts(ctypes.Structure):
+    _fields_ = [(n, f64) for n in ("two_pi", "pi", "w_ref", "l_ref", "rho", "cl", "p0", "pv", "st2", "k1", "p0pv",
+                                   "k4", "tw", "k6", "hl", "k9", "k10", "k11", "km2")] + \
+        [("system_params", f64 * 5)]
+
+
+def admit_record_len(nk: int) -> int:
+    """Doubles per request record of cbc_admit (CBC_ADMIT_RECORD)."""
+    return 5 + 3 * int(nk) + 64
+
+
 class CBCError(RuntimeError):
     """A C-ABI call returned a negative code."""
 
@@ -123,6 +134,8 @@ EXTRA_SIGNATURES: list = [
                                   ctypes.POINTER(cbc_work), i64, ctypes.POINTER(cbc_env_io), ctypes.POINTER(P)]),
     ("cbc_ensemble_solve_noalloc", i32, [P, ctypes.POINTER(cbc_spec), ctypes.POINTER(cbc_ensemble),
                                          ctypes.POINTER(cbc_work), i64, P]),
+    ("cbc_admit", i32, [P, ctypes.POINTER(cbc_ensemble), ctypes.POINTER(cbc_precompute_consts), P, i32, i32, i64,
+                        P]),
     ("cbc_plan_launch", i32, [P, P]),
     ("cbc_kernel_launches", i64, [P]),
     ("cbc_plan_destroy", i32, [P]),

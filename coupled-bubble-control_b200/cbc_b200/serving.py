@@ -1,37 +1,48 @@
-"""Continuous-batching solve server on one GPU.
+"""Continuous-batching solve server on one GPU, device-resident.
 
 Requests (one CKM1D system each: K bubbles, radii, drive, positions, span)
-arrive at any time.  The server keeps a device-resident slot pool per K
-bucket (a ragged ensemble preallocated once) and runs a loop of
+arrive at any time.  The server owns one preallocated ragged ensemble on the
+device -- a table of system slots, a pool of bubble rows and a pool of
+coupling storage -- and runs a loop of ticks:
 
-  1. admit  -- queued requests whose bucket has a free slot are written into
-               free slots (parameter precompute on the host, one batched
-               host->device copy per bucket),
-  2. advance -- one batched solve over all occupied slots with a bounded step
-               budget per system (``chunk_steps``); systems resume exactly where
-               the previous chunk stopped, so a request's result does not depend
-               on what else is in flight,
-  3. harvest -- statuses of the occupied slots come back (a few bytes per
-               slot); finished requests release their slot.
+  1. admit   -- queued requests, oldest first, are admitted while the pools
+                have room for them: a free slot, K contiguous bubble rows and
+                3 K^2 coupling elements (admission by device memory, any K
+                <= 32 in one pool).  The host only packs the raw requests into
+                a pinned staging buffer; one host->device copy, then the
+                parameter precompute and the initial state are written on the
+                GPU (cbc_admit, bit-identical to the host precompute);
+  2. advance -- one batched solve over every occupied slot for a slice of
+                device time (cbc_work.budget_ns): each warp steps its systems
+                until the slice ends, then stops them after their current step
+                (status -1, resumable bit for bit).  Oldest requests are
+                claimed first.  max_steps caps the steps a request accumulates
+                over all slices;
+  3. harvest -- the status and step counters of the slot table come back in
+                one asynchronous copy into pinned memory (8 bytes per slot);
+                finished requests release their slot and pool ranges.
 
-Requests that arrive while others are on the GPU are admitted as soon as
-slots free up and their work overlaps on the device with everything else in
-flight.  Latency = completion time - arrival time.  There is no reference
-counterpart (the reference only runs fixed batches through Model.solve); the
-per-system integration is the same kernel and arithmetic as every other path.
+State never leaves the GPU between slices; the host sees only statuses and,
+on request, the results of finished requests.  A request's result does not
+depend on what else is in flight (alone == in the mix, tests/test_serving.py).
+Latency = the end of the tick that saw the request finish - its arrival.
+No reference counterpart: the reference only runs fixed batches through
+Model.solve (models/model.py:108-162); the per-system integration is the same
+kernel and arithmetic as every other path.
 """
 from __future__ import annotations
 
+import ctypes
 import time
 from collections import deque
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import Dict, List, Optional
 
 import numpy as np
 
-from . import scenes
-from .ensemble import Ensemble, WorkList
-from .models import SolverSpec
+from . import _lib, admission, scenes
+from .admission import RangeAllocator
+from .models import SolverSpec, water
 
 
 @dataclass
@@ -44,139 +55,247 @@ class Request:
     X0: np.ndarray           # (K,) dimensionless positions
     span: float              # periods
     arrival: float = 0.0     # seconds (server clock)
+    admitted: float = -1.0
     done: float = -1.0
     slot: int = -1
+    status: int = 0
     result: Optional[Dict[str, np.ndarray]] = None
 
 
-class SolveServer:
-    """Slot pool: ``slots[K]`` systems of K bubbles for every K bucket."""
+# device bytes a request of K bubbles occupies in the pools (state + bubble
+# constants per bubble, coupling block, per-system rows and scalars)
+def request_bytes(K: int, nk: int = 2) -> int:
+    return 160 * K + 24 * K * K + (8 * 8 + 8 * 4 * nk + 8 * 7 + 4 * 6)
 
-    def __init__(self, slots: Dict[int, int], nk: int = 2, ac: str = "SW_A", freqs_khz=(25.0, 50.0),
-                 chunk_steps: int = 2048, max_steps: int = 1_000_000, solver_spec: Optional[SolverSpec] = None,
-                 device: int = 0, keep_results: bool = False):
+
+class SolveServer:
+    """Device-resident continuous batching over one slot table.
+
+    max_systems: slot-table size (requests in flight at most);
+    memory_bytes: device memory for the bubble-row and coupling pools
+    (default: enough for every slot to hold K = 16); slice_ms: device time
+    per advance.  ``slots`` (a dict K -> count) is accepted for callers of the
+    earlier per-bucket interface and only sizes the pools.
+    """
+
+    def __init__(self, slots: Optional[Dict[int, int]] = None, max_systems: int = 0, memory_bytes: int = 0,
+                 nk: int = 2, ac: str = "SW_A", freqs_khz=(25.0, 50.0), ref_freq_khz: float = 25.0,
+                 slice_ms: float = 2.0, chunk_steps: int = 0, max_steps: int = 1_000_000,
+                 solver_spec: Optional[SolverSpec] = None, device: int = 0, keep_results: bool = False):
         import torch
-        self.nk, self.ac, self.freqs = nk, ac, tuple(freqs_khz)
-        self.chunk_steps = int(chunk_steps)
+        self.nk, self.ac, self.freqs = int(nk), ac, tuple(float(f) for f in freqs_khz)
         self.max_steps = int(max_steps)
+        self.slice_ns = int(slice_ms * 1e6)
+        self.chunk_steps = int(chunk_steps)        # > 0: a step budget per advance instead of a time slice
         self.keep_results = keep_results
         self.device = device
-        self.tdev = torch.device("cuda", device)
-        ks = sorted(slots)
-        Ks = np.concatenate([np.full(slots[k], k, np.int32) for k in ks])
-        ns = Ks.size
-        # placeholder systems; every slot is (re)written at admission
-        sc = scenes.Scene(K=Ks, R0=[np.full(k, 5.0) for k in Ks], PA=np.zeros((nk, ns)),
-                          FR=np.tile(np.asarray(freqs_khz)[:, None], (1, ns)), PS=np.zeros((nk, ns)),
-                          X0=[np.linspace(-0.2, 0.2, k) if k > 1 else np.zeros(1) for k in Ks],
-                          t_end=np.zeros(ns), ac=ac)
-        self.ens = Ensemble.from_scene(sc, solver_spec=solver_spec, device=device)
-        self.ens.host["t_end"][:] = 0.0
-        self.ens.host["status"][:] = 1
-        self.ens.to_device()
-        self.bucket_of = {k: np.nonzero(Ks == k)[0] for k in ks}
-        self.free = {k: deque(self.bucket_of[k].tolist()) for k in ks}
+        self.solver_spec = solver_spec if solver_spec is not None else SolverSpec()
+        dev = torch.device("cuda", device)
+        if slots:
+            max_systems = max_systems or int(sum(slots.values()))
+            rows = int(sum(k * n for k, n in slots.items()))
+            coup = int(sum(3 * k * k * n for k, n in slots.items()))
+        else:
+            max_systems = max_systems or 16384
+            per = memory_bytes // max_systems if memory_bytes else 0
+            kcap = 16
+            if per:
+                while kcap > 1 and 160 * kcap + 24 * kcap * kcap > per:
+                    kcap //= 2
+            rows, coup = max_systems * kcap, max_systems * 3 * kcap * kcap
+        self.S = int(max_systems)
+        f64, i32, i64 = torch.float64, torch.int32, torch.int64
+        z = lambda n, dt: torch.zeros(n, dtype=dt, device=dev)   # noqa: E731
+        self.d = {
+            "bubble_offset": z(self.S, i64), "coupling_offset": z(self.S, i64),
+            "state": z((rows, 4), f64), "unit_params": z((rows, 16), f64),
+            "system_params": z((self.S, 8), f64), "control_params": z((self.S, 4 * self.nk), f64),
+            "coupling": z(max(coup, 1), f64), "t": z(self.S, f64), "t_end": z(self.S, f64),
+            "t_begin": z(self.S, f64), "h": z(self.S, f64), "event": z(self.S, f64),
+            "status": torch.ones(self.S, dtype=i32, device=dev), "steps": z(self.S, i32),
+            "rejected": z(self.S, i32), "conv_ok": z(self.S, i32), "conv_fail": z(self.S, i32),
+            "lin_iters": z(self.S, i64), "order": z(self.S, i32), "records": None,
+        }
+        self.rows = RangeAllocator(rows)
+        self.coup = RangeAllocator(coup)
+        self.free_slots = deque(range(self.S))
+        self.slot_K = np.zeros(self.S, np.int32)
         self.busy: Dict[int, Request] = {}
-        self.queue: Dict[int, deque] = {k: deque() for k in ks}
+        self.busy_order: List[int] = []             # slots in admission order
+        self.queue: deque = deque()
         self.completed: List[Request] = []
-        self.steps_done = 0
+        self.stream = torch.cuda.Stream(device=dev)
+        # pinned staging: request records, the work list, the status read-back
+        self.rl = _lib.admit_record_len(self.nk)
+        self.rec_cap = 4096
+        self.h_rec = torch.zeros((self.rec_cap, self.rl), dtype=f64).pin_memory()
+        self.d["records"] = torch.zeros((self.rec_cap, self.rl), dtype=f64, device=dev)
+        self.h_order = torch.zeros(self.S, dtype=i32).pin_memory()
+        self.h_status = torch.zeros(self.S, dtype=i32).pin_memory()
+        self.h_steps = torch.zeros(self.S, dtype=i32).pin_memory()
+        self.consts = admission.consts_struct(water(), ref_freq_khz)
+        self.ctx = _lib.default_context(device)
+        self.lib = _lib.lib()
+        self.abi = self._abi()
+        self.spec = self._spec()
+        self.ticks = 0
         self.t0 = time.perf_counter()
+
+    # ---- ABI structures (built once; the arrays never move) ----
+    def _abi(self) -> _lib.cbc_ensemble:
+        d = self.d
+        e = _lib.cbc_ensemble()
+        e.ns, e.nb = self.S, int(d["state"].shape[0])
+        e.up_stride, e.sp_stride, e.cp_stride = 16, 8, 4 * self.nk
+        for name in ("bubble_offset", "coupling_offset", "state", "unit_params", "system_params",
+                     "control_params", "coupling", "t", "t_end", "t_begin", "h", "event", "status",
+                     "steps", "rejected", "conv_ok", "conv_fail", "lin_iters"):
+            setattr(e, name, d[name].data_ptr())
+        return e
+
+    def _spec(self) -> _lib.cbc_spec:
+        s = self.solver_spec
+        return _lib.cbc_spec(self.S, 0, 0, 0, self.nk, _lib.AC_CODES[self.ac], _lib.DENSE_CODES[s.dense_mode],
+                             int(s.lin_max_iter), s.atol, s.rtol, s.min_step, s.max_step, s.lin_atol, s.lin_rtol,
+                             s.lin_relaxation, s.etol, s.col_threshold, _lib.LIN_CODES[s.lin_solver], 0)
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
 
     # ---- client side ----
     def submit(self, req: Request) -> None:
-        if req.K not in self.queue:
-            raise ValueError(f"no slot bucket for K={req.K}")
-        self.queue[req.K].append(req)
+        if not 1 <= req.K <= 32:
+            raise ValueError(f"K = {req.K}: 1..32 bubbles per request")
+        if len(req.PA) != self.nk or len(req.PS) != self.nk:
+            raise ValueError(f"PA and PS need {self.nk} harmonic components")
+        self.queue.append(req)
 
     # ---- loop ----
     def _admit(self) -> int:
         import torch
-        d, h = self.ens.dev, self.ens.host
-        admitted = 0
-        for k, q in self.queue.items():
-            n = min(len(q), len(self.free[k]))
-            if n == 0:
-                continue
-            reqs = [q.popleft() for _ in range(n)]
-            slots = np.asarray([self.free[k].popleft() for _ in range(n)], dtype=np.int64)
-            sc = scenes.Scene(K=np.full(n, k, np.int32), R0=[r.R0 for r in reqs],
-                              PA=np.stack([r.PA for r in reqs], 1), FR=np.tile(np.asarray(self.freqs)[:, None], (1, n)),
-                              PS=np.stack([r.PS for r in reqs], 1), X0=[r.X0 for r in reqs],
-                              t_end=np.asarray([r.span for r in reqs]), ac=self.ac)
-            part = Ensemble.from_scene(sc, solver_spec=self.ens.solver_spec)
-            rows = (h["bubble_offset"][slots][:, None] + np.arange(k)[None, :]).reshape(-1)
-            crow = (h["coupling_offset"][slots][:, None] + np.arange(3 * k * k)[None, :]).reshape(-1)
-            sl = torch.from_numpy(slots).to(self.tdev)
-            rw = torch.from_numpy(rows).to(self.tdev)
-            cr = torch.from_numpy(crow).to(self.tdev)
-            P = part.host
-            for name, idx in (("state", rw), ("unit_params", rw)):
-                d[name].index_copy_(0, idx, torch.from_numpy(P[name]).to(self.tdev))
-            d["coupling"].index_copy_(0, cr, torch.from_numpy(P["coupling"]).to(self.tdev))
-            for name in ("system_params", "control_params", "t", "t_end", "t_begin", "h", "event", "status",
-                         "steps", "rejected", "conv_ok", "conv_fail", "lin_iters"):
-                d[name].index_copy_(0, sl, torch.from_numpy(P[name]).to(self.tdev))
-            for r, s in zip(reqs, slots):
-                r.slot = int(s)
-                self.busy[int(s)] = r
-            admitted += n
-        return admitted
+        took: List[Request] = []
+        offs = []
+        while self.queue and self.free_slots and len(took) < self.rec_cap:
+            r = self.queue[0]
+            b = self.rows.alloc(r.K)
+            if b is None:
+                break
+            c = self.coup.alloc(3 * r.K * r.K)
+            if c is None:
+                self.rows.free(b, r.K)
+                break                               # oldest first: no overtaking
+            self.queue.popleft()
+            s = self.free_slots.popleft()
+            took.append(r)
+            offs.append((s, b, c))
+        if not took:
+            return 0
+        n = len(took)
+        rec = self.h_rec.numpy()
+        admission.pack_records([r.K for r in took], [o[0] for o in offs], [o[1] for o in offs],
+                               [o[2] for o in offs], [r.span for r in took],
+                               np.stack([r.PA for r in took]), np.tile(np.asarray(self.freqs), (n, 1)),
+                               np.stack([r.PS for r in took]), [r.R0 for r in took], [r.X0 for r in took], out=rec)
+        t = self.now()
+        with torch.cuda.stream(self.stream):
+            self.d["records"][:n].copy_(self.h_rec[:n], non_blocking=True)
+        self.ctx.check(self.lib.cbc_admit(self.ctx.handle, ctypes.byref(self.abi), ctypes.byref(self.consts),
+                                          self.d["records"].data_ptr(), n, self.nk,
+                                          int(self.d["coupling"].numel()),
+                                          ctypes.c_void_p(self.stream.cuda_stream)))
+        for r, (s, b, c) in zip(took, offs):
+            r.slot, r.admitted = s, t
+            r._ranges = (b, c)
+            self.slot_K[s] = r.K
+            self.busy[s] = r
+            self.busy_order.append(s)
+        return n
 
     def _advance(self) -> None:
-        slots = np.fromiter(self.busy.keys(), dtype=np.int64)
-        if slots.size == 0:
+        import torch
+        if not self.busy_order:
             return
-        K = self.ens.host["K"][slots]
-        ks = np.unique(K)
+        slots = np.asarray(self.busy_order, np.int32)
+        K = self.slot_K[slots]
+        ks = np.unique(K)[::-1]
         order, begins = [], [0]
-        for k in ks[::-1]:
-            sel = slots[K == k]
+        for k in ks:
+            sel = slots[K == k]                     # admission order inside the bucket
             order.append(sel)
             begins.append(begins[-1] + sel.size)
-        wl = WorkList(order=np.concatenate(order).astype(np.int32), bucket_K=ks[::-1].astype(np.int32),
-                      bucket_begin=np.asarray(begins, np.int32))
-        self.ens.solve(self.chunk_steps, work=wl)
+        o = np.concatenate(order)
+        self.h_order.numpy()[:o.size] = o
+        with torch.cuda.stream(self.stream):
+            self.d["order"][:o.size].copy_(self.h_order[:o.size], non_blocking=True)
+        bk = np.ascontiguousarray(ks, np.int32)
+        bb = np.asarray(begins, np.int32)
+        w = _lib.cbc_work()
+        w.order = self.d["order"].data_ptr()
+        w.nbuckets = int(bk.size)
+        w.bucket_K = bk.ctypes.data
+        w.bucket_begin = bb.ctypes.data
+        if self.chunk_steps > 0:
+            max_steps, w.steps_total = self.chunk_steps, 0
+        else:
+            max_steps, w.steps_total, w.budget_ns = self.max_steps, 1, self.slice_ns
+        self.ctx.check(self.lib.cbc_ensemble_solve(self.ctx.handle, ctypes.byref(self.spec), ctypes.byref(self.abi),
+                                                   ctypes.byref(w), int(max_steps),
+                                                   ctypes.c_void_p(self.stream.cuda_stream)))
 
     def _harvest(self) -> int:
         import torch
-        slots = np.fromiter(self.busy.keys(), dtype=np.int64)
-        if slots.size == 0:
+        if not self.busy:
             return 0
-        idx = torch.from_numpy(slots).to(self.tdev)
-        st = self.ens.dev["status"][idx].cpu().numpy()
-        steps = self.ens.dev["steps"][idx].cpu().numpy()
-        # -1: chunk budget spent, still running -- unless the request's total
-        # step budget is used up, then it finishes as MAX_STEPS_REACHED
-        finished = slots[(st != -1) | (steps >= self.max_steps)]
+        with torch.cuda.stream(self.stream):
+            self.h_status.copy_(self.d["status"], non_blocking=True)
+            self.h_steps.copy_(self.d["steps"], non_blocking=True)
+        self.stream.synchronize()
+        st = self.h_status.numpy()
+        steps = self.h_steps.numpy()
+        slots = np.asarray(self.busy_order, np.int64)
+        s_st, s_steps = st[slots], steps[slots]
+        # 0: not yet claimed; -1: stopped by the slice; else finished.  A
+        # step-budget chunk (chunk_steps) ends a request only at its own cap.
+        fin = (s_st != 0) & (s_st != -1) | (s_steps >= self.max_steps)
+        if not np.any(fin):
+            return 0
         tnow = self.now()
-        for s in finished:
+        done = set(slots[fin].tolist())
+        for s in slots[fin]:
             r = self.busy.pop(int(s))
             r.done = tnow
+            r.status = int(st[s])
             if self.keep_results:
                 r.result = self.result_of(int(s))
-            self.free[r.K].append(int(s))
+            b, c = r._ranges
+            self.rows.free(b, r.K)
+            self.coup.free(c, 3 * r.K * r.K)
+            self.free_slots.append(int(s))
             self.completed.append(r)
-        return int(finished.size)
+        self.busy_order = [s for s in self.busy_order if s not in done]
+        return len(done)
 
     def result_of(self, slot: int) -> Dict[str, np.ndarray]:
-        h = self.ens.host
-        k = int(h["K"][slot])
-        b0 = int(h["bubble_offset"][slot])
-        d = self.ens.dev
+        r = self.busy.get(slot)
+        k = int(self.slot_K[slot])
+        b0 = int(self.d["bubble_offset"][slot].item())
+        d = self.d
         return {"state": d["state"][b0:b0 + k].cpu().numpy(), "t": float(d["t"][slot]),
                 "status": int(d["status"][slot]), "steps": int(d["steps"][slot]), "h": float(d["h"][slot])}
 
     def step(self) -> int:
-        """One admit/advance/harvest iteration; returns completions."""
+        """One admit / advance / harvest tick; returns completions."""
         self._admit()
         self._advance()
+        self.ticks += 1
         return self._harvest()
 
     def idle(self) -> bool:
-        return not self.busy and all(len(q) == 0 for q in self.queue.values())
+        return not self.busy and not self.queue
+
+    def occupancy(self) -> Dict[str, float]:
+        return {"systems": len(self.busy), "rows_used": self.rows.used, "coupling_used": self.coup.used,
+                "queued": len(self.queue)}
 
 
 def latency_stats(done: List[Request]) -> Dict[str, float]:
@@ -185,3 +304,38 @@ def latency_stats(done: List[Request]) -> Dict[str, float]:
         return {}
     return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p95_ms": float(np.percentile(lat, 95) * 1e3),
             "p99_ms": float(np.percentile(lat, 99) * 1e3), "completed": int(lat.size)}
+
+
+def requests_from_scene(scene: scenes.Scene, arrivals: np.ndarray) -> List[Request]:
+    """Requests of a (ragged) scene with the given arrival times (s)."""
+    return [Request(rid=i, K=int(scene.K[i]), R0=np.asarray(scene.R0[i]), PA=scene.PA[:, i].copy(),
+                    PS=scene.PS[:, i].copy(), X0=np.asarray(scene.X0[i]), span=float(scene.t_end[i]),
+                    arrival=float(arrivals[i])) for i in range(scene.ns)]
+
+
+def serve_stream(server: SolveServer, reqs: List[Request], duration_s: float, drain: bool = False) -> Dict:
+    """Plays an arrival-time-stamped request stream against the server's
+    clock for `duration_s` seconds (then drains if asked) and reports latency
+    percentiles of the completed requests and the achieved throughput
+    against the offered load."""
+    pending = deque(sorted(reqs, key=lambda r: r.arrival))
+    server.t0 = time.perf_counter()
+    offered = sum(r.span for r in reqs if r.arrival < duration_s)
+    while True:
+        t = server.now()
+        while pending and pending[0].arrival <= t:
+            server.submit(pending.popleft())
+        server.step()
+        if t >= duration_s and (not drain or server.idle()):
+            break
+        if not pending and server.idle():
+            break
+    wall = server.now()
+    done = server.completed
+    adv = sum(r.span for r in done if r.status == 1)
+    out = latency_stats(done)
+    out.update({"duration_s": duration_s, "wall_s": wall, "submitted": sum(1 for r in reqs if r.arrival < duration_s),
+                "completed": len(done), "in_flight": len(server.busy), "queued": len(server.queue),
+                "offered_system_periods_per_s": offered / duration_s,
+                "completed_system_periods_per_s": adv / wall, "ticks": server.ticks})
+    return out

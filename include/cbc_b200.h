@@ -178,24 +178,25 @@ int32_t cbc_solve(cbc_context* ctx, const cbc_spec* spec, const cbc_buffers* buf
  *   dense_state                      (ndo, nb, 4)    sample-major; 16-byte aligned
  *   steps, rejected, conv_ok, conv_fail (ns) i32, lin_iters (ns) i64: optional
  * The spec's ns, ups and tile fields are ignored; its solver fields, nk, ac,
- * ndo and dense_mode apply to every system.  The solvers only read
- * control_params and t_end; a plan made by cbc_env_plan_create also writes
- * them (the actions and the step's end time, see cbc_env_io), which is why
- * they are not const. */
+ * ndo and dense_mode apply to every system.  The solvers only read the
+ * offsets, parameters, coupling, t_begin and t_end; cbc_admit writes all of them for
+ * the slots it fills and a plan made by cbc_env_plan_create writes
+ * control_params and t_end (the actions and the step's end time, see
+ * cbc_env_io), which is why they are not const. */
 typedef struct cbc_ensemble {
   int32_t ns;
   int32_t up_stride, sp_stride, cp_stride;
   int64_t nb;
-  const int64_t* bubble_offset;
-  const int64_t* coupling_offset;
+  int64_t* bubble_offset;
+  int64_t* coupling_offset;
   double* state;
-  const double* unit_params;
-  const double* system_params;
+  double* unit_params;
+  double* system_params;
   double* control_params;
-  const double* coupling;
+  double* coupling;
   double* t;
   double* t_end;
-  const double* t_begin;
+  double* t_begin;
   double* h;
   double* event;
   int32_t* status;
@@ -300,6 +301,40 @@ int32_t cbc_plan_create(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemb
                         const cbc_work* work, int64_t max_steps, cbc_plan** out);
 int32_t cbc_plan_launch(cbc_plan* plan, void* stream);
 int32_t cbc_plan_destroy(cbc_plan* plan);
+
+/* ---- device-side admission (parameter precompute on the GPU) ---------------
+ * Scalar constants of the precompute, evaluated on the host from the
+ * material properties and the reference frequency f (Hz), exactly as
+ * cbc_b200.models.ckm1d.precompute_constants does: two_pi = 2 pi,
+ * w_ref = two_pi f, l_ref = c / f, st2 = 2 sigma, k1 = 1 - 3 gamma,
+ * p0pv = P0 - Pv, k4 = 4 mu / rho, tw = two_pi / w_ref,
+ * k6 = tw^2 / c / rho, hl = l_ref / 2, k9 = two_pi / rho, k10 = 2 two_pi / 3,
+ * k11 = 6 two_pi mu, km2 = (18 mu / rho) tw, system_params the 5 per-system
+ * constants (3 gamma, 1 / w_ref, l_ref / two_pi, c, 1 / rho / c), pi = pi. */
+typedef struct cbc_precompute_consts {
+  double two_pi, pi, w_ref, l_ref, rho, cl, p0, pv;
+  double st2, k1, p0pv, k4, tw, k6, hl, k9, k10, k11, km2;
+  double system_params[5];
+} cbc_precompute_consts;
+
+/* Doubles per request record of cbc_admit for nk harmonics:
+ * [K, slot, bubble_offset, coupling_offset, span, PA[nk] (bar), FR[nk] (kHz),
+ *  PS[nk] (phase / pi), R0[32] (um, first K used), X0[32] (positions in
+ *  units of the reference wavelength, first K used)]. */
+#define CBC_ADMIT_RECORD(nk) (5 + 3 * (nk) + 64)
+
+/* Writes n raw requests (device array `records`, n * CBC_ADMIT_RECORD(nk)
+ * doubles) into their slots of the ensemble: bubble_offset / coupling_offset
+ * of the slot, the 13 bubble constants, the per-system and control
+ * parameters, the 3 K x K coupling block, the initial state (R = 1, X = X0,
+ * U = V = 0), t = 0, t_end = span, t_begin = 0, h = 1e-6, event = -1,
+ * status 0 and zero counters.  One warp per request.  Bit-identical to the
+ * host precompute (reference models/ckm1d.py:133-202, model.py:180-225),
+ * which it replaces for served requests.  coupling_len: doubles in
+ * ens->coupling; a record whose slot or ranges fall outside the ensemble is
+ * skipped.  No reference counterpart on the GPU. */
+int32_t cbc_admit(cbc_context* ctx, const cbc_ensemble* ens, const cbc_precompute_consts* consts,
+                  const double* records, int32_t n, int32_t nk, int64_t coupling_len, void* stream);
 
 /* ---- vec-env step ------------------------------------------------------------
  * Device buffers of one environment step around the batched solve (uniform K,

@@ -13,7 +13,7 @@ from cbc_b200 import _lib
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 STRUCTS = [_lib.cbc_spec, _lib.cbc_buffers, _lib.cbc_solve_stats, _lib.cbc_ensemble, _lib.cbc_work,
-           _lib.cbc_env_io]
+           _lib.cbc_env_io, _lib.cbc_precompute_consts]
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="no host C compiler")

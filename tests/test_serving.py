@@ -49,3 +49,27 @@ def test_alone_equals_in_mix(cuda):
         assert a["steps"] == b["steps"] and a["h"] == b["h"]
     stats = latency_stats(list(mix.values()))
     assert stats["completed"] == 60 and stats["p99_ms"] >= stats["p50_ms"] > 0
+
+
+def test_admission_by_memory_and_fifo(cuda):
+    """Pools sized for two K = 8 requests: the third waits for memory (and a
+    later K = 2 request does not overtake it); everything completes."""
+    from cbc_b200.serving import SolveServer as S
+    srv = S(max_systems=8, memory_bytes=0, slice_ms=1.0, keep_results=False)
+    srv.rows = type(srv.rows)(16)                       # room for 16 bubble rows
+    srv.coup = type(srv.coup)(2 * 3 * 64)               # and two K = 8 coupling blocks
+    reqs = make_requests(40, seed=9)
+    k8 = [r for r in reqs if r.K == 8][:3]
+    k2 = [r for r in reqs if r.K == 2][:1]
+    for r in k8 + k2:
+        r.arrival = 0.0
+        srv.submit(r)
+    srv._admit()
+    assert len(srv.busy) == 2 and len(srv.queue) == 2 and srv.queue[0] is k8[2]
+    it = 0
+    while not srv.idle():
+        srv.step()
+        it += 1
+        assert it < 100000
+    assert {r.rid for r in srv.completed} == {r.rid for r in k8 + k2}
+    assert srv.rows.used == 0 and srv.coup.used == 0 and len(srv.free_slots) == 8
