@@ -367,6 +367,56 @@ def env_step_latency(dev_index: int, n_steps: int = 128, warmup: int = 3):
             "env_system_periods_per_s": float(1024 * 5.0 / (t.mean() * 1e-3))}
 
 
+def large_k_measure(dev_index: int, ns: int = 16384, periods: float = 1.0, peak_tflops: float = 0.0):
+    """Large-K dense output (K = 32, one warp per system, 64 samples per
+    period): one batched solve of `ns` systems over `periods` periods from
+    resident inputs.  Reports system-periods/s, the FP64 roofline numerator
+    and the HBM rate of the trajectory writes (dense samples + times)."""
+    import torch
+    from cbc_b200 import scenes
+    from cbc_b200.ensemble import Ensemble
+    sc = scenes.large_k(ns=ns, K=32, periods=periods, samples_per_period=64, seed=4)
+    ens = Ensemble.from_scene(sc, device=dev_index).to_device()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    ens.solve(MAX_STEPS)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    res = ens.to_host()
+    adv = float(np.sum(res["t"] - ens.host["t"]))
+    samples = int(np.sum(res["dense_index"]))
+    dense_bytes = samples * 32 * 4 * 8 + samples * 8
+    flops = flop_count(res["K"], res["steps"], res["lin_iters"])
+    out = {"workload": f"large_k_{ns}x32_{periods:g}periods_64spp", "systems": ns, "K": 32,
+           "periods": periods, "dense_samples": int(sc.ndo), "value": adv / (ms * 1e-3), "unit": UNIT,
+           "ms": ms, "status_counts": {int(k): int(v) for k, v in zip(*np.unique(res["status"], return_counts=True))},
+           "trajectory_bytes": dense_bytes, "trajectory_hbm_gbs": dense_bytes / (ms * 1e-3) / 1e9,
+           "bytes_per_system_period": dense_bytes / max(adv, 1e-30),
+           "achieved_tflops": flops / (ms * 1e-3) / 1e12,
+           "note": "span reduced from 200 to %g periods: 200 periods of 16,384 systems write 216 GB of "
+                   "samples (more than the GPU holds) and take hours of FP64 work" % periods}
+    if peak_tflops > 0:
+        out["roofline_frac"] = out["achieved_tflops"] / peak_tflops
+    return out
+
+
+def served_measure(dev_index: int, rate_hz: float, duration_s: float, seed: int = 3):
+    """Served solve stream: Poisson arrivals at `rate_hz`, K ~ U{2,4,8,16},
+    spans U[1,50] periods, played for `duration_s` seconds against the
+    device-resident server (requests admitted by free pool memory)."""
+    from cbc_b200 import scenes
+    from cbc_b200.serving import SolveServer, requests_from_scene, serve_stream
+    n = int(rate_hz * duration_s * 1.2) + 16
+    arrivals, sc = scenes.served_stream(duration_s=duration_s, rate_hz=rate_hz, seed=seed, max_requests=n)
+    reqs = requests_from_scene(sc, arrivals)
+    srv = SolveServer(max_systems=65536, memory_bytes=2 << 30, slice_ms=2.0, device=dev_index)
+    out = serve_stream(srv, reqs, duration_s)
+    out.update({"rate_hz": rate_hz, "K": [2, 4, 8, 16], "span_periods": [1, 50]})
+    return out
+
+
 def run_b200(args):
     import torch
     rank, world, local = dist_env()
@@ -511,6 +561,11 @@ def run_b200(args):
         if env_lat:
             line["env_step_latency"] = env_lat
         line["alone_latency"] = alone_latency(scene, local, "richardson")
+        if args.served:
+            line["served"] = {"offered_20k": served_measure(local, 20000.0, args.serve_seconds),
+                              "sustainable_1k": served_measure(local, 1000.0, args.serve_seconds)}
+        if args.large_k:
+            line["large_k"] = large_k_measure(local, peak_tflops=peak)
         if lu:
             lu["roofline_frac"] = lu["achieved_tflops"] / peak
             line["lin_solver_lu"] = lu
@@ -534,6 +589,11 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-env", dest="env", action="store_false")
+    ap.add_argument("--no-served", dest="served", action="store_false",
+                    help="skip the served-stream measurement (Poisson 20k req/s and 1k req/s)")
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--no-large-k", dest="large_k", action="store_false",
+                    help="skip the large-K dense-output measurement")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="skip the autotuner (default launch shape for every K)")
     ap.add_argument("--no-lu", dest="lu", action="store_false",

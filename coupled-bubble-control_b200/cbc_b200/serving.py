@@ -121,7 +121,7 @@ class SolveServer:
         self.free_slots = deque(range(self.S))
         self.slot_K = np.zeros(self.S, np.int32)
         self.busy: Dict[int, Request] = {}
-        self.busy_order: List[int] = []             # slots in admission order
+        self.busy_order = np.zeros(0, np.int32)     # occupied slots in admission order
         self.queue: deque = deque()
         self.completed: List[Request] = []
         self.stream = torch.cuda.Stream(device=dev)
@@ -139,6 +139,7 @@ class SolveServer:
         self.abi = self._abi()
         self.spec = self._spec()
         self.ticks = 0
+        torch.cuda.synchronize(device)     # the pools are initialised before the server stream uses them
         self.t0 = time.perf_counter()
 
     # ---- ABI structures (built once; the arrays never move) ----
@@ -208,14 +209,14 @@ class SolveServer:
             r._ranges = (b, c)
             self.slot_K[s] = r.K
             self.busy[s] = r
-            self.busy_order.append(s)
+        self.busy_order = np.concatenate([self.busy_order, np.asarray([o[0] for o in offs], np.int32)])
         return n
 
     def _advance(self) -> None:
         import torch
-        if not self.busy_order:
+        if self.busy_order.size == 0:
             return
-        slots = np.asarray(self.busy_order, np.int32)
+        slots = self.busy_order
         K = self.slot_K[slots]
         ks = np.unique(K)[::-1]
         order, begins = [], [0]
@@ -252,7 +253,7 @@ class SolveServer:
         self.stream.synchronize()
         st = self.h_status.numpy()
         steps = self.h_steps.numpy()
-        slots = np.asarray(self.busy_order, np.int64)
+        slots = self.busy_order
         s_st, s_steps = st[slots], steps[slots]
         # 0: not yet claimed; -1: stopped by the slice; else finished.  A
         # step-budget chunk (chunk_steps) ends a request only at its own cap.
@@ -260,8 +261,8 @@ class SolveServer:
         if not np.any(fin):
             return 0
         tnow = self.now()
-        done = set(slots[fin].tolist())
-        for s in slots[fin]:
+        done = slots[fin]
+        for s in done:
             r = self.busy.pop(int(s))
             r.done = tnow
             r.status = int(st[s])
@@ -272,8 +273,8 @@ class SolveServer:
             self.coup.free(c, 3 * r.K * r.K)
             self.free_slots.append(int(s))
             self.completed.append(r)
-        self.busy_order = [s for s in self.busy_order if s not in done]
-        return len(done)
+        self.busy_order = slots[~fin]
+        return int(done.size)
 
     def result_of(self, slot: int) -> Dict[str, np.ndarray]:
         r = self.busy.get(slot)

@@ -104,7 +104,7 @@ def test_admit_skips_records_outside_the_ensemble(cuda):
     ref, blank = _ensemble_with_slots(sc)
     blank.to_device()
     h = ref.host
-    rec = admission.pack_records([int(sc.K[0])] * 3, [0, 25, 1], [h["bubble_offset"][0], 0, 10 ** 9],
+    rec = admission.pack_records(sc.K[:3], [0, 25, 1], [h["bubble_offset"][0], 0, 10 ** 9],
                                  [h["coupling_offset"][0], 0, 0], [1.0] * 3, sc.PA.T[:3], sc.FR.T[:3],
                                  sc.PS.T[:3], sc.R0[:3], sc.X0[:3])
     d_rec = torch.from_numpy(rec).cuda()
