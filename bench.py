@@ -190,7 +190,8 @@ def cpu_baseline(scene, seconds: float = 12.0, nthreads: int = 0, seed: int = 99
 def workload_config(args, world: int) -> dict:
     """The workload both arms report (the reference arm times a bounded CPU
     sample of it, described in its cpu_baseline.sample)."""
-    return {"workload": f"mixed_k_{args.ns}", "ns_per_gpu": args.ns, "K": [2, 3, 4, 6, 8],
+    wname = f"mixed_k_{args.ns}" + (f"_only_K{args.only_k}" if args.only_k > 0 else "")
+    return {"workload": wname, "ns_per_gpu": args.ns, "K": [2, 3, 4, 6, 8],
             "K_weights": [0.4, 0.2, 0.2, 0.1, 0.1], "span_periods": [5, 50], "rtol": 1e-9,
             "atol": 1e-9, "max_steps": args.max_steps, "field": "SW_A 25+50 kHz",
             "l2": "256 MiB buffer written before every step", "parallelism": f"replicas{world}",
@@ -432,6 +433,8 @@ def run_b200(args):
     from cbc_b200.ensemble import Ensemble
 
     scene = scenes.mixed_k(ns=args.ns, seed=rank_seed(rank))
+    if args.only_k > 0:      # profiling cases: one K bucket of the workload, filling the GPU
+        scene = scenes.subset(scene, np.nonzero(scene.K == args.only_k)[0])
     ens = Ensemble.from_scene(scene, device=local)
     ens.to_device()
     tune_info = None
@@ -594,6 +597,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--no-large-k", dest="large_k", action="store_false",
                     help="skip the large-K dense-output measurement")
+    ap.add_argument("--only-k", type=int, default=0,
+                    help="keep only the systems of this K (profiling a single bucket that fills the GPU)")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="skip the autotuner (default launch shape for every K)")
     ap.add_argument("--no-lu", dest="lu", action="store_false",

@@ -64,7 +64,12 @@ class cbc_work(ctypes.Structure):
 
 class cbc_env_io(ctypes.Structure):
     _fields_ = [("actions", P), ("n_act", i32), ("act_stride", i32), ("act_scale", f64), ("obs", P),
-                ("failed", P), ("K", i32), ("pad", i32), ("t_span", f64), ("h0", f64)]
+                ("failed", P), ("K", i32), ("pad", i32), ("t_span", f64), ("h0", f64)] + \
+        [(n, P) for n in ("targets", "rewards", "terminated", "time_outs", "done", "algo_steps", "total_rewards",
+                          "final_obs", "episode_return", "episode_len", "reset_count")] + \
+        [(n, f64) for n in ("position_tolerance", "r_dnorm", "reward_exp", "w_dist", "w_intensity", "pos_reward",
+                            "neg_reward", "min_distance", "max_distance", "domain_lo", "domain_hi")] + \
+        [("episode_length", i32), ("pad2", i32), ("seed", ctypes.c_uint64)]
 
 
 class cbc_precompute_consts(ctypes.Structure):
@@ -136,6 +141,7 @@ EXTRA_SIGNATURES: list = [
                                          ctypes.POINTER(cbc_work), i64, P]),
     ("cbc_admit", i32, [P, ctypes.POINTER(cbc_ensemble), ctypes.POINTER(cbc_precompute_consts), P, i32, i32, i64,
                         P]),
+    ("cbc_env_reset", i32, [P, ctypes.POINTER(cbc_ensemble), ctypes.POINTER(cbc_env_io), P, P]),
     ("cbc_plan_launch", i32, [P, P]),
     ("cbc_kernel_launches", i64, [P]),
     ("cbc_plan_destroy", i32, [P]),

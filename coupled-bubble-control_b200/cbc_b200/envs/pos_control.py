@@ -7,14 +7,16 @@ positions and radii as the observation, target positions, reward and
 termination as in the reference (``get_rewards`` :792-813,
 ``check_termination`` :772-789, ``advance_time`` :816-826,
 ``final_termination`` :830-853), and random scene resets
-(``SceneGenerator._random_uniform_position_1D`` :176-234).
+(``SceneGenerator._random_uniform_position_1D`` :176-234, ``reset_envs``
+:583-614).
 
 One ``step`` is one CUDA-graph launch (``cbc_env_plan_create``): action ->
-control parameters, time reset, the batched integration of ``time_step_length``
-periods for every env, and the float32 observation written straight into
-``self.obs`` (a torch tensor the caller can keep; no copy).  The state stays
-on the device between steps.  Reward, termination and resets are a handful of
-torch ops on the same stream.
+control parameters and time reset (prologue kernel), the batched integration
+of ``time_step_length`` periods for every env, and one epilogue kernel that
+writes the float32 observation straight into ``self.obs``, computes reward
+and termination, and resets the envs that finished (new positions and
+targets drawn on the device).  No torch op and no host synchronisation is
+part of a step; the state stays on the device.
 """
 from __future__ import annotations
 
@@ -27,42 +29,70 @@ from .. import _lib, scenes
 from ..ensemble import Ensemble, make_work_list
 from ..models import SolverSpec
 
+_M64 = (1 << 64) - 1
+
+
+def _splitmix64(z: np.ndarray) -> np.ndarray:
+    z = (z + np.uint64(0x9E3779B97F4A7C15)) & np.uint64(_M64)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
 
 class SceneGenerator:
-    """Random chains of bubbles inside [domain_min + margin, domain_max - margin]
-    with neighbour gaps in [min_distance, max_distance] (reference
-    SceneGenerator, envs/bubble_1D_pos_control.py:46-249, 'random' positions,
-    'center' alignment)."""
+    """Random chains of K bubbles inside [domain_min + margin, domain_max -
+    margin]: K - 1 gaps of min_distance plus uniform extras up to
+    max_distance - min_distance, scaled down to fit, centred (reference
+    SceneGenerator, envs/bubble_1D_pos_control.py:46-249, 'random'
+    positions, 'center' alignment).  The uniform draws are a counter-based
+    hash (SplitMix64) of (seed, env, reset count, stream, draw), so the
+    device epilogue (csrc/vecenv.cu) and this host restatement produce the
+    same scenes."""
 
     def __init__(self, num_bubbles: int, min_distance: float = 0.05, max_distance: float = 0.9,
-                 margin: float = 0.05, domain_min: float = -0.5, domain_max: float = 0.5, seed: int = 42,
-                 device="cuda"):
-        import torch
-        self.K = num_bubbles
-        self.min_distance, self.max_distance = min_distance, max_distance
+                 margin: float = 0.05, domain_min: float = -0.5, domain_max: float = 0.5, seed: int = 42):
+        self.K = int(num_bubbles)
+        self.min_distance, self.max_distance = float(min_distance), float(max_distance)
         self.lo, self.hi = domain_min + margin, domain_max - margin
-        self.gen = torch.Generator(device=device)
-        self.gen.manual_seed(seed)
-        self.device = device
-        avail = self.hi - self.lo
-        if (self.K - 1) * min_distance > avail:
-            raise ValueError(f"Cannot fit: the scene needs {(self.K - 1) * min_distance:.2f}, domain is {avail:.2f}")
+        self.seed = int(seed) & _M64
+        if (self.K - 1) * min_distance > self.hi - self.lo:
+            raise ValueError(f"Cannot fit: the scene needs {(self.K - 1) * min_distance:.2f}, "
+                             f"domain is {self.hi - self.lo:.2f}")
 
-    def positions(self, n: int, dtype=None):
-        import torch
-        dtype = dtype or torch.float64
-        gaps_n = self.K - 1
+    def uniform(self, env: np.ndarray, count: np.ndarray, which: int, j: int) -> np.ndarray:
+        with np.errstate(over="ignore"):
+            key = (np.uint64(self.seed) ^ (env.astype(np.uint64) * np.uint64(0xD1B54A32D192ED03))
+                   ^ (count.astype(np.uint64) * np.uint64(0xABC98388FB8FAC03))
+                   ^ np.uint64(((which * 64 + j) * 0x8CB92BA72F3D8DD7) & _M64))
+            return (_splitmix64(key) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+    def positions(self, env, count, which: int = 0) -> np.ndarray:
+        """(n, K) positions for envs `env` at their reset counts `count`
+        (which = 0: bubble positions, 1: targets)."""
+        env = np.atleast_1d(np.asarray(env, np.int64))
+        count = np.broadcast_to(np.asarray(count, np.int64), env.shape)
+        n, K = env.size, self.K
+        if K == 1:
+            return np.full((n, 1), 0.5 * (self.lo + self.hi))
         avail = self.hi - self.lo
-        if gaps_n == 0:
-            return torch.full((n, 1), 0.5 * (self.lo + self.hi), dtype=dtype, device=self.device)
         room = self.max_distance - self.min_distance
-        limit = avail - gaps_n * self.min_distance
-        extras = torch.rand((n, gaps_n), dtype=dtype, device=self.device, generator=self.gen) * room
-        scale = (limit / extras.sum(dim=1).clamp(min=1e-12)).clamp(max=1.0)
-        gaps = extras * scale.unsqueeze(-1) + self.min_distance
-        remaining = avail - gaps.sum(dim=1)
-        offset = self.lo + 0.5 * remaining.unsqueeze(-1)
-        return torch.cat([offset, offset + torch.cumsum(gaps, dim=1)], dim=1)
+        limit = avail - (K - 1) * self.min_distance
+        with np.errstate(over="ignore"):
+            ext = np.stack([self.uniform(env, count, which, j) * room for j in range(K - 1)], 1)
+        ssum = np.zeros(n)
+        for j in range(K - 1):
+            ssum = ssum + ext[:, j]
+        sc = np.minimum(limit / np.maximum(ssum, 1e-12), 1.0)
+        gsum = np.zeros(n)
+        gaps = np.empty_like(ext)
+        for j in range(K - 1):
+            gaps[:, j] = ext[:, j] * sc + self.min_distance
+            gsum = gsum + gaps[:, j]
+        out = np.empty((n, K))
+        out[:, 0] = self.lo + 0.5 * (avail - gsum)
+        for j in range(K - 1):
+            out[:, j + 1] = out[:, j] + gaps[:, j]
+        return out
 
 
 class CKM1DVecEnv:
@@ -91,7 +121,7 @@ class CKM1DVecEnv:
         self.pos_reward, self.neg_reward = positive_terminal_reward, negative_terminal_reward
         self.device = device
         self.tdev = torch.device("cuda", device)
-        self.scenes = SceneGenerator(self.K, seed=seed, device=self.tdev)
+        self.scenes = SceneGenerator(self.K, seed=seed)
         nk = len(freqs_khz)
         # physics: one uniform-K ensemble, initial PA (1, 0) bar as in the reference env defaults
         sc = scenes.Scene(K=np.full(self.num_envs, self.K, np.int32),
@@ -103,13 +133,23 @@ class CKM1DVecEnv:
                           t_end=np.full(self.num_envs, self.time_step_length), ac=acoustic_field)
         self.ens = Ensemble.from_scene(sc, solver_spec=solver_spec, device=device)
         self.ens.to_device()
-        d = self.ens.dev
-        self.actions = torch.zeros((self.num_envs, nk), dtype=torch.float32, device=self.tdev)
-        self.obs = torch.zeros((self.num_envs, 2 * self.K), dtype=torch.float32, device=self.tdev)
-        self.failed = torch.zeros(self.num_envs, dtype=torch.uint8, device=self.tdev)
-        self.targets = torch.zeros((self.num_envs, self.K), dtype=torch.float32, device=self.tdev)
-        self.algo_steps = torch.zeros(self.num_envs, dtype=torch.long, device=self.tdev)
-        self.total_rewards = torch.zeros(self.num_envs, dtype=torch.float32, device=self.tdev)
+        n = self.num_envs
+        f32 = torch.float32
+        z = lambda shape, dt: torch.zeros(shape, dtype=dt, device=self.tdev)   # noqa: E731
+        self.actions = z((n, nk), f32)
+        self.obs = z((n, 2 * self.K), f32)
+        self.failed = z(n, torch.uint8)
+        self.targets = z((n, self.K), f32)
+        self.rewards = z(n, f32)
+        self.terminated = z(n, torch.uint8)
+        self.time_outs = z(n, torch.uint8)
+        self.done = z(n, torch.uint8)
+        self.algo_steps = z(n, torch.int32)
+        self.total_rewards = z(n, f32)
+        self.final_obs = z((n, 2 * self.K), f32)
+        self.episode_return = z(n, f32)
+        self.episode_len = z(n, torch.int32)
+        self.reset_count = z(n, torch.int64)
         io = _lib.cbc_env_io()
         io.actions = self.actions.data_ptr()
         io.n_act = nk
@@ -120,6 +160,18 @@ class CKM1DVecEnv:
         io.K = self.K
         io.t_span = self.time_step_length
         io.h0 = 1e-6                   # advance_time resets the step to 1e-6 (:816-826)
+        for name in ("targets", "rewards", "terminated", "time_outs", "done", "algo_steps", "total_rewards",
+                     "final_obs", "episode_return", "episode_len", "reset_count"):
+            setattr(io, name, getattr(self, name).data_ptr())
+        io.position_tolerance = position_tolerance
+        io.r_dnorm = self.r_dnorm
+        io.reward_exp = reward_exp
+        io.w_dist, io.w_intensity = float(rewards_weights[0]), float(rewards_weights[1])
+        io.pos_reward, io.neg_reward = positive_terminal_reward, negative_terminal_reward
+        g = self.scenes
+        io.min_distance, io.max_distance, io.domain_lo, io.domain_hi = g.min_distance, g.max_distance, g.lo, g.hi
+        io.episode_length = self.episode_length
+        io.seed = g.seed
         self._io = io
         wl = make_work_list(self.ens.host["K"], np.full(self.num_envs, self.time_step_length))
         self._w, self._keep = self.ens.work(wl)
@@ -130,66 +182,37 @@ class CKM1DVecEnv:
                                                       ctypes.byref(self._e), ctypes.byref(self._w),
                                                       int(max_steps), ctypes.byref(io), ctypes.byref(h)))
         self.plan = h.value
-        # bubble rows of each env, for resets by index
-        self._rows = torch.as_tensor(self.ens.host["bubble_offset"], device=self.tdev).unsqueeze(1) + \
-            torch.arange(self.K, device=self.tdev).unsqueeze(0)
+        torch.cuda.synchronize(device)
 
     # ---- resets ----
-    def _write_scene(self, env_ids):
-        import torch
-        n = env_ids.numel()
-        pos = self.scenes.positions(n)
-        tgt = self.scenes.positions(n)
-        st = self.ens.dev["state"]
-        rows = self._rows[env_ids].reshape(-1)
-        fresh = torch.zeros((rows.numel(), 4), dtype=torch.float64, device=self.tdev)
-        fresh[:, 0] = 1.0
-        fresh[:, 1] = pos.reshape(-1)
-        st.index_copy_(0, rows, fresh)
-        self.targets.index_copy_(0, env_ids, tgt.to(torch.float32))
-        self.obs[env_ids, :self.K] = pos.to(torch.float32)
-        self.obs[env_ids, self.K:] = 1.0
-        self.algo_steps[env_ids] = 0
-        self.total_rewards[env_ids] = 0.0
-
     def reset(self) -> Tuple[object, Dict]:
+        """New scenes for every env (device kernel, the same draws and
+        formulas as the step's in-graph resets)."""
         import torch
-        self._write_scene(torch.arange(self.num_envs, device=self.tdev))
+        st = torch.cuda.current_stream(self.device)
+        self.ctx.check(_lib.lib().cbc_env_reset(self.ctx.handle, ctypes.byref(self._e), ctypes.byref(self._io),
+                                                None, ctypes.c_void_p(st.cuda_stream)))
         return self.obs, {}
 
     # ---- step ----
     def step_physics(self, stream=None) -> None:
-        """Action -> control parameters, integrate, observation (one graph launch)."""
+        """One environment step for every env (one graph launch)."""
         import torch
         st = stream if stream is not None else torch.cuda.current_stream(self.device)
         self.ctx.check(_lib.lib().cbc_plan_launch(self.plan, ctypes.c_void_p(st.cuda_stream)))
 
     def step(self, actions=None):
-        import torch
+        """Returns (obs, rewards, terminated, time_outs, info), all device
+        tensors written by the step's graph.  info['done'] marks the envs
+        that finished in this step and were reset; their last observation,
+        return and length are in info['final_observation'],
+        info['episode_return'] and info['episode_length'] (valid where done)."""
         if actions is not None:
             self.actions.copy_(actions)
         self.step_physics()
-        x = self.obs[:, :self.K]
-        failure = self.failed.bool()
-        td = (self.targets - x).abs()
-        success = torch.all(td <= self.position_tolerance, dim=1)
-        td = td.masked_fill(td < self.position_tolerance, 0.0)
-        dist = (td * self.r_dnorm).clamp(min=0.0).pow(self.reward_exp).mean(dim=1)
-        intensity = self.actions.pow(2.0).sum(dim=1).sqrt()
-        rewards = (-self.weights[0] * dist - self.weights[1] * intensity + self.neg_reward * failure.float()
-                   + self.pos_reward * success.float())
-        self.total_rewards += rewards
-        self.algo_steps += 1
-        terminated = failure | success
-        time_outs = self.algo_steps >= self.episode_length
-        done = torch.nonzero(terminated | time_outs).flatten()
-        info = {}
-        if done.numel() > 0:
-            info = {"final_observation": self.obs[done].clone(), "dones": done,
-                    "episode_return": self.total_rewards[done].clone(),
-                    "episode_length": self.algo_steps[done].clone()}
-            self._write_scene(done)
-        return self.obs, rewards, terminated, time_outs, info
+        info = {"done": self.done, "final_observation": self.final_obs, "episode_return": self.episode_return,
+                "episode_length": self.episode_len}
+        return self.obs, self.rewards, self.terminated, self.time_outs, info
 
     def close(self) -> None:
         if getattr(self, "plan", None):

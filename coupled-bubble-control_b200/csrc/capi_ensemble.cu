@@ -20,6 +20,7 @@ namespace cbc {
 
 int32_t enqueue_env_begin(cbc_context* ctx, const cbc_ensemble* e, const cbc_env_io* io, cudaStream_t st);
 int32_t enqueue_env_end(cbc_context* ctx, const cbc_ensemble* e, const cbc_env_io* io, cudaStream_t st);
+bool env_epilogue_fields_ok(const cbc_env_io* io);
 
 static int32_t check_ensemble(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* e, const cbc_work* w) {
   if (!spec) return fail(ctx, CBC_E_INVALID, "spec is NULL");
@@ -345,6 +346,9 @@ int32_t cbc_env_plan_create(cbc_context* ctx, const cbc_spec* spec, const cbc_en
         io->K < 1 || io->K > 32 || (long long)io->K * e->ns != e->nb || !(io->t_span > 0.0) || !(io->h0 > 0.0))
       return fail(ctx, CBC_E_INVALID, "env io: need actions, obs, 0 <= n_act <= cp_stride, a uniform K with "
                                       "ns * K == nb, t_span > 0 and h0 > 0");
+    if (io->rewards && !env_epilogue_fields_ok(io))
+      return fail(ctx, CBC_E_INVALID, "env io: the reward epilogue needs every one of its buffers, "
+                                      "episode_length >= 1 and domain_hi > domain_lo");
   }
   DeviceGuard dg(ctx->device);
   cbc_plan* p = new (std::nothrow) cbc_plan();

@@ -357,7 +357,47 @@ typedef struct cbc_env_io {
   int32_t pad;
   double t_span;
   double h0;
+  /* ---- optional fused epilogue: reward, termination and resets ----------
+   * Used when rewards != NULL (then every pointer below must be set).  After
+   * the observation, for every env s (reference get_rewards :792-813,
+   * check_termination :772-789, final_termination :830-853), in float32:
+   *   td_i = |targets[s][i] - x_i|, success = all td_i <= tol,
+   *   td_i = 0 where td_i < tol, dist = mean_i (td_i * r_dnorm)^reward_exp,
+   *   intensity = sqrt(sum_a actions[s][a]^2),
+   *   rewards[s] = -w_dist dist - w_intensity intensity + neg_reward failed
+   *                + pos_reward success,
+   *   total_rewards[s] += rewards[s], algo_steps[s] += 1,
+   *   terminated[s] = failed | success, time_outs[s] = algo_steps >= episode_length.
+   * A finished env (terminated or timed out) keeps final_obs[s] = its
+   * observation, episode_return[s] / episode_len[s] its totals, and is reset
+   * in place (reset_envs :583-614): new positions and targets from the scene
+   * generator (reference SceneGenerator :183-242; uniform draws from a
+   * counter-based hash of (seed, env, reset_count[s])), state R = 1, X = the
+   * positions, U = V = 0, observation [positions, 1], totals 0,
+   * reset_count[s] += 1.  done[s] = 1 marks the envs reset in this step. */
+  float* targets;          /* (ns, K) */
+  float* rewards;          /* (ns) */
+  uint8_t* terminated;     /* (ns) */
+  uint8_t* time_outs;      /* (ns) */
+  uint8_t* done;           /* (ns) */
+  int32_t* algo_steps;     /* (ns) */
+  float* total_rewards;    /* (ns) */
+  float* final_obs;        /* (ns, 2K) */
+  float* episode_return;   /* (ns) */
+  int32_t* episode_len;    /* (ns) */
+  int64_t* reset_count;    /* (ns) */
+  double position_tolerance, r_dnorm, reward_exp, w_dist, w_intensity, pos_reward, neg_reward;
+  double min_distance, max_distance, domain_lo, domain_hi;   /* scene generator (margins applied) */
+  int32_t episode_length;
+  int32_t pad2;
+  uint64_t seed;
 } cbc_env_io;
+
+/* Resets the envs s with mask[s] != 0 (every env when mask is NULL) exactly
+ * as the fused epilogue resets a finished env (scene generator draws, state,
+ * observation, totals, reset_count).  Needs the epilogue fields of io. */
+int32_t cbc_env_reset(cbc_context* ctx, const cbc_ensemble* ens, const cbc_env_io* io, const uint8_t* mask,
+                      void* stream);
 
 /* A plan whose graph is env prologue -> batched solve -> env epilogue; one
  * cbc_plan_launch is one environment step for every env (io == NULL gives

@@ -35,3 +35,17 @@ def test_plain_and_large_k_workloads():
     lk = scenes.large_k(ns=8, K=32, periods=200.0, samples_per_period=64, seed=4)
     assert np.all(lk.K == 32) and lk.ndo == 12801
     _check_positions(lk, -0.5, 0.5)
+
+
+def test_env_scene_generator_draws():
+    """Host restatement of the env's device scene generator: chains inside
+    the domain with gaps >= min_distance, different per env and per reset."""
+    from cbc_b200.envs import SceneGenerator
+    g = SceneGenerator(4, seed=5)
+    p = g.positions(np.arange(200), 0, 0)
+    assert p.shape == (200, 4)
+    gaps = np.diff(p, axis=1)
+    assert np.all(gaps >= g.min_distance - 1e-12) and np.all(p >= g.lo - 1e-12) and np.all(p <= g.hi + 1e-12)
+    assert not np.array_equal(p, g.positions(np.arange(200), 1, 0))
+    assert not np.array_equal(p, g.positions(np.arange(200), 0, 1))
+    assert np.array_equal(p, SceneGenerator(4, seed=5).positions(np.arange(200), 0, 0))

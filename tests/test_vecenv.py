@@ -1,5 +1,9 @@
 """Vec-env step on the GPU (one graph launch: action -> control parameters,
-time reset, batched integration, float32 observation) against the oracle."""
+time reset, batched integration, then one epilogue kernel for the float32
+observation, reward, termination and the resets of finished envs) against
+the oracle, a torch restatement of the reference's reward and termination
+(envs/bubble_1D_pos_control.py:772-813) and the host restatement of the
+scene generator."""
 import numpy as np
 import pytest
 
@@ -36,11 +40,64 @@ def test_env_step_matches_oracle(cuda):
     oracle.solve_ref_layout(spec, ref, 1_000_000)
     x = ref["actual_state"][1].astype(np.float32)
     R = ref["actual_state"][0].astype(np.float32)
-    got = env.obs.cpu().numpy()
-    assert np.array_equal(got[:, :4], x) and np.array_equal(got[:, 4:], R)
+    done = env.done.cpu().numpy().astype(bool)
+    seen = np.where(done[:, None], env.final_obs.cpu().numpy(), env.obs.cpu().numpy())
+    assert np.array_equal(seen[:, :4], x) and np.array_equal(seen[:, 4:], R)
     assert np.array_equal(env.failed.cpu().numpy(), (ref["status_flags"] != 1).astype(np.uint8))
-    after = env.ens.to_host()
-    assert np.array_equal(after["state"].reshape(48, 4, 4), np.transpose(ref["actual_state"], (1, 2, 0)))
+    after = env.ens.to_host()["state"].reshape(48, 4, 4)
+    want = np.transpose(ref["actual_state"], (1, 2, 0))
+    assert np.array_equal(after[~done], want[~done])
+    env.close()
+
+
+def _torch_reward(x, targets, failed, actions, tol=0.01, dnorm=0.2, exp=0.5, w=(1.0, 0.0), pos=10.0, neg=-10.0):
+    """The reference's reward and termination (get_rewards :792-813,
+    check_termination :772-789) in torch float32."""
+    import torch
+    td = (targets - x).abs()
+    success = torch.all(td <= tol, dim=1)
+    td = td.masked_fill(td < tol, 0.0)
+    dist = (td * (1.0 / dnorm)).clamp(min=0.0).pow(exp).mean(dim=1)
+    intensity = actions.pow(2.0).sum(dim=1).sqrt()
+    reward = -w[0] * dist - w[1] * intensity + neg * failed.float() + pos * success.float()
+    return reward, failed | success
+
+
+def test_reward_termination_and_resets(cuda):
+    import torch
+    from cbc_b200.envs import CKM1DVecEnv, SceneGenerator
+    n, K = 96, 4
+    env = CKM1DVecEnv(num_envs=n, num_bubbles=K, time_step_length=0.03, episode_length=2, seed=11,
+                      position_tolerance=0.05)
+    env.reset()
+    torch.cuda.synchronize()
+    gen = SceneGenerator(K, seed=11)
+    ids = np.arange(n)
+    p0 = gen.positions(ids, 0, 0)
+    assert np.array_equal(env.ens.to_host()["state"].reshape(n, K, 4)[:, :, 1], p0)
+    assert np.array_equal(env.targets.cpu().numpy(), gen.positions(ids, 0, 1).astype(np.float32))
+    assert np.array_equal(env.obs.cpu().numpy()[:, :K], p0.astype(np.float32))
+    act = torch.rand((n, 2), device="cuda", generator=torch.Generator(device="cuda").manual_seed(3)) * 1.2
+    for step in range(3):
+        tgt = env.targets.clone()
+        steps_before = env.algo_steps.clone()
+        obs, rew, term, tout, info = env.step(act)
+        torch.cuda.synchronize()
+        done = info["done"].bool()
+        x = torch.where(done[:, None], info["final_observation"], obs)[:, :K]
+        r_ref, term_ref = _torch_reward(x, tgt, env.failed.bool(), act, tol=0.05)
+        assert torch.allclose(rew, r_ref, rtol=1e-6, atol=1e-6)
+        assert torch.equal(term.bool(), term_ref)
+        assert torch.equal(tout.bool(), steps_before + 1 >= 2)
+        assert torch.equal(done, term.bool() | tout.bool())
+        d = done.cpu().numpy()
+        if d.any():
+            cnt = env.reset_count.cpu().numpy()
+            assert np.all(cnt[d] >= 2)
+            newpos = gen.positions(ids[d], cnt[d] - 1, 0)
+            assert np.array_equal(obs.cpu().numpy()[d, :K], newpos.astype(np.float32))
+            assert np.all(env.algo_steps.cpu().numpy()[d] == 0)
+            assert np.array_equal(info["episode_length"].cpu().numpy()[d], (steps_before + 1).cpu().numpy()[d])
     env.close()
 
 
