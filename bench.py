@@ -193,7 +193,7 @@ def workload_config(args, world: int) -> dict:
     wname = f"mixed_k_{args.ns}" + (f"_only_K{args.only_k}" if args.only_k > 0 else "")
     return {"workload": wname, "ns_per_gpu": args.ns, "K": [2, 3, 4, 6, 8],
             "K_weights": [0.4, 0.2, 0.2, 0.1, 0.1], "span_periods": [5, 50], "rtol": 1e-9,
-            "atol": 1e-9, "max_steps": args.max_steps, "field": "SW_A 25+50 kHz",
+            "atol": 1e-9, "max_steps": args.max_steps, "field": "SW_A 25+50 kHz", "lin_solver": args.lin_solver,
             "l2": "256 MiB buffer written before every step", "parallelism": f"replicas{world}",
             "schedule": args.schedule}
 
@@ -435,7 +435,8 @@ def run_b200(args):
     scene = scenes.mixed_k(ns=args.ns, seed=rank_seed(rank))
     if args.only_k > 0:      # profiling cases: one K bucket of the workload, filling the GPU
         scene = scenes.subset(scene, np.nonzero(scene.K == args.only_k)[0])
-    ens = Ensemble.from_scene(scene, device=local)
+    from cbc_b200.models import SolverSpec
+    ens = Ensemble.from_scene(scene, solver_spec=SolverSpec(lin_solver=args.lin_solver), device=local)
     ens.to_device()
     tune_info = None
     if args.tune:
@@ -482,7 +483,7 @@ def run_b200(args):
     kern_ms = [a.elapsed_time(b) for a, b in ev]
     res = ens.to_host()
     adv = float(np.sum(res["t"] - ens.host["t"]))
-    flops = flop_count(res["K"], res["steps"], res["lin_iters"])
+    flops = flop_count(res["K"], res["steps"], res["lin_iters"], args.lin_solver)
     status = {int(k): int(v) for k, v in zip(*np.unique(res["status"], return_counts=True))}
 
     total_ms_all, work_all = job_totals(total_ms, adv * args.steps, pg, dev)
@@ -597,6 +598,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--no-large-k", dest="large_k", action="store_false",
                     help="skip the large-K dense-output measurement")
+    ap.add_argument("--lin-solver", default="richardson", choices=["richardson", "lu"],
+                    help="implicit-coupling solver of the headline arm (richardson: the reference's)")
     ap.add_argument("--only-k", type=int, default=0,
                     help="keep only the systems of this K (profiling a single bucket that fills the GPU)")
     ap.add_argument("--no-tune", dest="tune", action="store_false",

@@ -114,9 +114,9 @@ __device__ __forceinline__ Geo make_geo(int K, int slots = 32) {
   const int lane = threadIdx.x & 31;
   g.lane = lane;
   g.K = K;
-  g.G = 32 / K < slots ? 32 / K : slots;
+  g.G = 32 / K;                          // layout of the group regions (unchanged by slots)
   const int grp = lane / K;
-  g.valid = grp < g.G;
+  g.valid = grp < g.G && grp < slots;    // groups past `slots` stay idle
   g.grp = g.valid ? grp : 0;
   g.base = g.valid ? grp * K : lane;
   g.li = g.valid ? lane - grp * K : 0;
