@@ -265,16 +265,16 @@ def plain_per_k(scene, dev, solver_spec=None):
     return adv / total, total
 
 
-def alone_latency(scene, dev_index: int, lin_solver: str, attempts: int = 3000):
+def alone_latency(scene, dev_index: int, lin_solver: str, attempts: int = 3000, ks=(2, 4, 8)):
     """Per-attempt latency (us) of single systems running alone (one warp on
-    an otherwise idle GPU): for K = 2, 4 and 8, the longest-span system of
+    an otherwise idle GPU): for each K in `ks`, the longest-span system of
     that K in the workload, `attempts` step attempts from its initial state."""
     import torch
     from cbc_b200 import scenes
     from cbc_b200.ensemble import Ensemble
     from cbc_b200.models import SolverSpec
     out = {}
-    for k in (2, 4, 8):
+    for k in ks:
         sel = np.nonzero(scene.K == k)[0]
         if sel.size == 0:
             continue
@@ -368,7 +368,7 @@ def env_step_latency(dev_index: int, n_steps: int = 128, warmup: int = 3):
             "env_system_periods_per_s": float(1024 * 5.0 / (t.mean() * 1e-3))}
 
 
-def large_k_measure(dev_index: int, ns: int = 16384, periods: float = 1.0, peak_tflops: float = 0.0):
+def large_k_measure(dev_index: int, ns: int = 16384, periods: float = 0.5, peak_tflops: float = 0.0):
     """Large-K dense output (K = 32, one warp per system, 64 samples per
     period): one batched solve of `ns` systems over `periods` periods from
     resident inputs.  Reports system-periods/s, the FP64 roofline numerator
@@ -582,6 +582,30 @@ def run_b200(args):
         pg.destroy_process_group()
 
 
+def run_alone(args):
+    """Per-attempt latency of single systems alone, both coupling solvers:
+    K = 1..8 from the mixed-K workload's distributions, 16 and 32 from
+    uniform scenes.  One JSON line."""
+    import torch
+    from cbc_b200 import scenes
+    torch.cuda.set_device(0)
+    mix = scenes.mixed_k(ns=args.ns, seed=1)
+    extra = []
+    for k in (1, 5, 7, 16, 32):
+        u = scenes.uniform(k, ns=4, periods=3.0, seed=90 + k, pa_hi=1.2 if k > 8 else 1.5,
+                           x_range=(-0.5, 0.5) if k > 8 else (-0.25, 0.25))
+        extra.append(u)
+    sc = mix
+    for u in extra:
+        sc = scenes.Scene(K=np.concatenate([sc.K, u.K]), R0=sc.R0 + u.R0, PA=np.hstack([sc.PA, u.PA]),
+                          FR=np.hstack([sc.FR, u.FR]), PS=np.hstack([sc.PS, u.PS]), X0=sc.X0 + u.X0,
+                          t_end=np.concatenate([sc.t_end, u.t_end]), ac="SW_A")
+    ks = (1, 2, 3, 4, 5, 6, 7, 8, 16, 32)
+    out = {"workload": "alone_latency", "unit": "us per step attempt",
+           "richardson": alone_latency(sc, 0, "richardson", ks=ks), "lu": alone_latency(sc, 0, "lu", ks=ks)}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -598,6 +622,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--no-large-k", dest="large_k", action="store_false",
                     help="skip the large-K dense-output measurement")
+    ap.add_argument("--workload", default="mixed_k", choices=["mixed_k", "alone"],
+                    help="alone: only the single-system step latency of both coupling solvers")
     ap.add_argument("--lin-solver", default="richardson", choices=["richardson", "lu"],
                     help="implicit-coupling solver of the headline arm (richardson: the reference's)")
     ap.add_argument("--only-k", type=int, default=0,
@@ -616,7 +642,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    if args.impl == "reference":
+    if args.workload == "alone":
+        run_alone(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)

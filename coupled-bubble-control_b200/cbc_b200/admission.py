@@ -53,10 +53,12 @@ def pack_records(K: Sequence[int], slot: Sequence[int], bubble_offset: Sequence[
     rec[:, 5 + nk:5 + 2 * nk] = FR
     rec[:, 5 + 2 * nk:5 + 3 * nk] = PS
     base = 5 + 3 * nk
-    for i in range(n):
-        k = int(K[i])
-        rec[i, base:base + k] = R0[i]
-        rec[i, base + 32:base + 32 + k] = X0[i]
+    rec[:, base:] = 0.0
+    Ka = np.asarray(K, np.int64)
+    for k in np.unique(Ka):                    # one stacked copy per bubble count
+        idx = np.nonzero(Ka == k)[0]
+        rec[idx, base:base + k] = np.stack([R0[i] for i in idx])
+        rec[idx, base + 32:base + 32 + k] = np.stack([X0[i] for i in idx])
     return rec
 
 

@@ -114,7 +114,7 @@ class SolveServer:
             "t_begin": z(self.S, f64), "h": z(self.S, f64), "event": z(self.S, f64),
             "status": torch.ones(self.S, dtype=i32, device=dev), "steps": z(self.S, i32),
             "rejected": z(self.S, i32), "conv_ok": z(self.S, i32), "conv_fail": z(self.S, i32),
-            "lin_iters": z(self.S, i64), "order": z(self.S, i32), "records": None,
+            "lin_iters": z(self.S, i64),
         }
         self.rows = RangeAllocator(rows)
         self.coup = RangeAllocator(coup)
@@ -126,13 +126,17 @@ class SolveServer:
         self.completed: List[Request] = []
         self.stream = torch.cuda.Stream(device=dev)
         # pinned staging: request records, the work list, the status read-back
+        # (two of each: the host fills one while the GPU may still read the other)
         self.rl = _lib.admit_record_len(self.nk)
         self.rec_cap = 4096
-        self.h_rec = torch.zeros((self.rec_cap, self.rl), dtype=f64).pin_memory()
-        self.d["records"] = torch.zeros((self.rec_cap, self.rl), dtype=f64, device=dev)
-        self.h_order = torch.zeros(self.S, dtype=i32).pin_memory()
-        self.h_status = torch.zeros(self.S, dtype=i32).pin_memory()
-        self.h_steps = torch.zeros(self.S, dtype=i32).pin_memory()
+        self.h_rec = [torch.zeros((self.rec_cap, self.rl), dtype=f64).pin_memory() for _ in range(2)]
+        self.d_rec = [torch.zeros((self.rec_cap, self.rl), dtype=f64, device=dev) for _ in range(2)]
+        self.d_order = [torch.zeros(self.S, dtype=i32, device=dev) for _ in range(2)]
+        self.h_order = [torch.zeros(self.S, dtype=i32).pin_memory() for _ in range(2)]
+        self.h_status = [torch.zeros(self.S, dtype=i32).pin_memory() for _ in range(2)]
+        self.h_steps = [torch.zeros(self.S, dtype=i32).pin_memory() for _ in range(2)]
+        self.readback = [None, None]             # (event, slots advanced) per buffer
+        self.pipelined = True
         self.consts = admission.consts_struct(water(), ref_freq_khz)
         self.ctx = _lib.default_context(device)
         self.lib = _lib.lib()
@@ -192,16 +196,17 @@ class SolveServer:
         if not took:
             return 0
         n = len(took)
-        rec = self.h_rec.numpy()
+        par = self.ticks & 1
+        rec = self.h_rec[par].numpy()
         admission.pack_records([r.K for r in took], [o[0] for o in offs], [o[1] for o in offs],
                                [o[2] for o in offs], [r.span for r in took],
                                np.stack([r.PA for r in took]), np.tile(np.asarray(self.freqs), (n, 1)),
                                np.stack([r.PS for r in took]), [r.R0 for r in took], [r.X0 for r in took], out=rec)
         t = self.now()
         with torch.cuda.stream(self.stream):
-            self.d["records"][:n].copy_(self.h_rec[:n], non_blocking=True)
+            self.d_rec[par][:n].copy_(self.h_rec[par][:n], non_blocking=True)
         self.ctx.check(self.lib.cbc_admit(self.ctx.handle, ctypes.byref(self.abi), ctypes.byref(self.consts),
-                                          self.d["records"].data_ptr(), n, self.nk,
+                                          self.d_rec[par].data_ptr(), n, self.nk,
                                           int(self.d["coupling"].numel()),
                                           ctypes.c_void_p(self.stream.cuda_stream)))
         for r, (s, b, c) in zip(took, offs):
@@ -225,13 +230,14 @@ class SolveServer:
             order.append(sel)
             begins.append(begins[-1] + sel.size)
         o = np.concatenate(order)
-        self.h_order.numpy()[:o.size] = o
+        par = self.ticks & 1
+        self.h_order[par].numpy()[:o.size] = o
         with torch.cuda.stream(self.stream):
-            self.d["order"][:o.size].copy_(self.h_order[:o.size], non_blocking=True)
+            self.d_order[par][:o.size].copy_(self.h_order[par][:o.size], non_blocking=True)
         bk = np.ascontiguousarray(ks, np.int32)
         bb = np.asarray(begins, np.int32)
         w = _lib.cbc_work()
-        w.order = self.d["order"].data_ptr()
+        w.order = self.d_order[par].data_ptr()
         w.nbuckets = int(bk.size)
         w.bucket_K = bk.ctypes.data
         w.bucket_begin = bb.ctypes.data
@@ -243,17 +249,33 @@ class SolveServer:
                                                    ctypes.byref(w), int(max_steps),
                                                    ctypes.c_void_p(self.stream.cuda_stream)))
 
-    def _harvest(self) -> int:
+    def _readback(self) -> None:
+        """Enqueues the copy of the slot table's statuses and step counters
+        into this tick's pinned buffers (after the tick's solve)."""
         import torch
-        if not self.busy:
-            return 0
+        par = self.ticks & 1
+        if self.busy_order.size == 0:
+            self.readback[par] = None
+            return
         with torch.cuda.stream(self.stream):
-            self.h_status.copy_(self.d["status"], non_blocking=True)
-            self.h_steps.copy_(self.d["steps"], non_blocking=True)
-        self.stream.synchronize()
-        st = self.h_status.numpy()
-        steps = self.h_steps.numpy()
-        slots = self.busy_order
+            self.h_status[par].copy_(self.d["status"], non_blocking=True)
+            self.h_steps[par].copy_(self.d["steps"], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(self.stream)
+        self.readback[par] = (ev, self.busy_order.copy())
+
+    def _harvest(self, par: int) -> int:
+        """Releases the requests that had finished by the read-back `par`."""
+        rb = self.readback[par]
+        if rb is None:
+            return 0
+        ev, slots = rb
+        self.readback[par] = None
+        ev.synchronize()
+        if slots.size == 0:
+            return 0
+        st = self.h_status[par].numpy()
+        steps = self.h_steps[par].numpy()
         s_st, s_steps = st[slots], steps[slots]
         # 0: not yet claimed; -1: stopped by the slice; else finished.  A
         # step-budget chunk (chunk_steps) ends a request only at its own cap.
@@ -262,6 +284,8 @@ class SolveServer:
             return 0
         tnow = self.now()
         done = slots[fin]
+        if self.keep_results:
+            self.stream.synchronize()            # results read after the slice in flight
         for s in done:
             r = self.busy.pop(int(s))
             r.done = tnow
@@ -273,7 +297,7 @@ class SolveServer:
             self.coup.free(c, 3 * r.K * r.K)
             self.free_slots.append(int(s))
             self.completed.append(r)
-        self.busy_order = slots[~fin]
+        self.busy_order = self.busy_order[~np.isin(self.busy_order, done)]
         return int(done.size)
 
     def result_of(self, slot: int) -> Dict[str, np.ndarray]:
@@ -285,14 +309,36 @@ class SolveServer:
                 "status": int(d["status"][slot]), "steps": int(d["steps"][slot]), "h": float(d["h"][slot])}
 
     def step(self) -> int:
-        """One admit / advance / harvest tick; returns completions."""
+        """One admit / advance / read-back tick; returns completions.
+
+        Pipelined: the tick enqueues its solve and status read-back, then
+        harvests the previous tick's read-back while the GPU works on this
+        one, so the host's bookkeeping overlaps the device time.  A request
+        is therefore released one tick after the slice that finished it
+        (its slot idles through that slice; results are unaffected)."""
         self._admit()
         self._advance()
+        self._readback()
+        par = self.ticks & 1
         self.ticks += 1
-        return self._harvest()
+        if self.pipelined:
+            return self._harvest(par ^ 1)
+        return self._harvest(par)
+
+    def drain(self) -> int:
+        """Harvests every outstanding read-back."""
+        return self._harvest(0) + self._harvest(1)
+
+    def advanced_system_periods(self) -> float:
+        """Simulated time advanced so far by every request in flight or done."""
+        done = sum(r.span if r.status == 1 else 0.0 for r in self.completed)
+        if self.busy_order.size == 0:
+            return done
+        t = self.d["t"].cpu().numpy()
+        return done + float(np.sum(t[self.busy_order]))
 
     def idle(self) -> bool:
-        return not self.busy and not self.queue
+        return not self.busy and not self.queue and self.readback[0] is None and self.readback[1] is None
 
     def occupancy(self) -> Dict[str, float]:
         return {"systems": len(self.busy), "rows_used": self.rows.used, "coupling_used": self.coup.used,
@@ -331,12 +377,15 @@ def serve_stream(server: SolveServer, reqs: List[Request], duration_s: float, dr
             break
         if not pending and server.idle():
             break
+    server.drain()
     wall = server.now()
     done = server.completed
     adv = sum(r.span for r in done if r.status == 1)
+    advanced = server.advanced_system_periods()
     out = latency_stats(done)
     out.update({"duration_s": duration_s, "wall_s": wall, "submitted": sum(1 for r in reqs if r.arrival < duration_s),
                 "completed": len(done), "in_flight": len(server.busy), "queued": len(server.queue),
                 "offered_system_periods_per_s": offered / duration_s,
-                "completed_system_periods_per_s": adv / wall, "ticks": server.ticks})
+                "completed_system_periods_per_s": adv / wall,
+                "advanced_system_periods_per_s": advanced / wall, "ticks": server.ticks})
     return out

@@ -33,6 +33,7 @@
 #pragma once
 
 #include <stdint.h>
+#include <string.h>
 #include <utility>
 #include "cbc_math.h"
 
@@ -405,50 +406,42 @@ __device__ __forceinline__ void residual_smem(const Geo& g, const double* m, dou
 //   R_i: x_i + cpf0_i sum_j (A_ij vr_j + B_ij vt_j) = b0_i
 //   T_i: x_{K+i} + sum_j (C_ij vr_j + D_ij vt_j)    = b1_i
 // Gauss-Jordan elimination with partial pivoting, column c = 0..2K-1:
-//   p   = the not-yet-pivot row with the largest |a[r][c]| (NaN ranks below
-//         every number, ties go to the smaller row index; a warp-shuffle
-//         argmax over the system's lanes);
+//   p   = the not-yet-pivot row with the largest pivot key (piv_key32: |a[r][c]|
+//         at 2^-13 relative resolution, NaN lowest, ties to the smaller row;
+//         a warp-shuffle max-reduction over the system's lanes);
 //   rp  = 1 / a[p][c];  pk[k] = a[p][k] for k = c+1..2K (k = 2K: right side);
 //   every row r: l = (r == p) ? 0 : a[r][c] * rp,  a[r][k] = fma(-l, pk[k], a[r][k]).
 // Pivot rows are eliminated too (Gauss-Jordan), so x_c = a[p_c][2K] * rp_c
 // with no triangular back-substitution pass.  ok = every pivot nonzero and
 // finite.  oracle/ckm1d_oracle.cpp (lu_solve) performs the same operations.
-constexpr int NO_ROW = 1 << 20;
-
-__device__ __forceinline__ double piv_key(double v, int r) {
-  return r >= NO_ROW ? -2.0 : (v != v ? -1.0 : fabs(v));
+// Pivot key of row r (0 <= r < 128) for column c: the high 32 bits of
+// |a[r][c]| (sign, exponent and 20 mantissa bits) with the low 7 bits replaced
+// by 127 - r.  The pivot is the row with the largest key: the largest
+// magnitude at 2^-13 relative resolution, ties to the smaller row; NaN ranks
+// below every number and rows that are already pivots have key 0.  One 32-bit
+// integer per row, so the argmax over a system's lanes is a max-reduction of
+// single shuffles.
+__host__ __device__ inline unsigned piv_key32(double v, int r, bool pivoted) {
+  unsigned long long b;
+  memcpy(&b, &v, sizeof b);
+  b &= 0x7FFFFFFFFFFFFFFFull;
+  unsigned hi = (unsigned)(b >> 32);
+  if (b > 0x7FF0000000000000ull) hi = 0u;    // NaN
+  return pivoted ? 0u : ((hi & ~127u) | (unsigned)(127 - r));
 }
-__device__ __forceinline__ bool piv_better(double va, int ra, double vb, int rb) {
-  const double ka = piv_key(va, ra), kb = piv_key(vb, rb);
-  return ka > kb || (ka == kb && ra < rb);
-}
 
-// Argmax of (value, row) over the group, the same total order in every lane.
+// Maximum of a key over the group (any K), the same in every lane.
 template <int KB>
-__device__ __forceinline__ void group_argmax(double& v, int& r, const Geo& g) {
+__device__ __forceinline__ unsigned group_max_u32(unsigned k, const Geo& g) {
 #pragma unroll
   for (int w = 1; w < KB; w <<= 1) {
     if (w < g.K) {
       const int q = (g.li ^ w) & ~(w - 1);
-      const int src = g.base + (q < g.K ? q : g.li);
-      const double vo = shfl(v, src);
-      const int ro = __shfl_sync(FULL, r, src);
-      if (q < g.K && piv_better(vo, ro, v, r)) {
-        v = vo;
-        r = ro;
-      }
+      const unsigned o = __shfl_sync(FULL, k, g.base + (q < g.K ? q : g.li));
+      if (q < g.K) k = o > k ? o : k;
     }
   }
-}
-
-// Candidate row of this lane for column c: the better of its rows that are
-// not pivots yet.
-__device__ __forceinline__ void lane_candidate(double vR, double vT, bool pR, bool pT, int li, int K, double& v,
-                                               int& r) {
-  const int rR = pR ? NO_ROW : li, rT = pT ? NO_ROW : K + li;
-  const bool takeR = piv_better(vR, rR, vT, rT);
-  v = takeR ? vR : vT;
-  r = takeR ? rR : rT;
+  return k;
 }
 
 // Register rows, exact K <= 8 known at compile time (every index static: the
@@ -467,14 +460,14 @@ __device__ __forceinline__ void lu_column(const Geo& g, double (&rR)[2 * KC], do
                                           double& hT, LuTrack& t) {
   constexpr int K = KC, N = 2 * KC;
   const int li = g.li;
-  double piv;
-  int p;
-  lane_candidate(rR[C], rT[C], t.pR, t.pT, li, K, piv, p);
-  group_argmax<(KC <= 2 ? 2 : (KC <= 4 ? 4 : 8))>(piv, p, g);
-  t.ok = t.ok && (piv != 0.0) && cbcm::isfinite_(piv);
-  const double rp = 1.0 / piv;
+  const unsigned kR = piv_key32(rR[C], li, t.pR), kT = piv_key32(rT[C], K + li, t.pT);
+  const unsigned km = group_max_u32<(KC <= 2 ? 2 : (KC <= 4 ? 4 : 8))>(kR > kT ? kR : kT, g);
+  const int p = 127 - (int)(km & 127u);
   const bool ps = p >= K;
   const int src = g.base + (ps ? p - K : p);
+  const double piv = shfl(ps ? rT[C] : rR[C], src);
+  t.ok = t.ok && (piv != 0.0) && cbcm::isfinite_(piv);
+  const double rp = 1.0 / piv;
   const bool meR = (p == li), meT = (p == K + li);
   t.pR = t.pR || meR;
   t.pT = t.pT || meT;
@@ -484,15 +477,33 @@ __device__ __forceinline__ void lu_column(const Geo& g, double (&rR)[2 * KC], do
   t.rpT = (C == K + li) ? rp : t.rpT;
   const double lR = meR ? 0.0 : rR[C] * rp;
   const double lT = meT ? 0.0 : rT[C] * rp;
+  // The pivot row is almost always the diagonal row C (the matrix is the
+  // identity plus the coupling terms): when it is for every system of the
+  // warp, its owner lane and row are compile-time constants and the row is
+  // broadcast without selects.  Both branches move the same values.
+  if (__all_sync(FULL, (p == C) || !g.valid)) {
+    constexpr bool DS = C >= K;
+    const int dsrc = g.base + (DS ? C - K : C);
 #pragma unroll
-  for (int k = C + 1; k < N; ++k) {
-    const double pk = shfl(ps ? rT[k] : rR[k], src);
-    rR[k] = fma(-lR, pk, rR[k]);
-    rT[k] = fma(-lT, pk, rT[k]);
+    for (int k = C + 1; k < N; ++k) {
+      const double pk = shfl(DS ? rT[k] : rR[k], dsrc);
+      rR[k] = fma(-lR, pk, rR[k]);
+      rT[k] = fma(-lT, pk, rT[k]);
+    }
+    const double ph = shfl(DS ? hT : hR, dsrc);
+    hR = fma(-lR, ph, hR);
+    hT = fma(-lT, ph, hT);
+  } else {
+#pragma unroll
+    for (int k = C + 1; k < N; ++k) {
+      const double pk = shfl(ps ? rT[k] : rR[k], src);
+      rR[k] = fma(-lR, pk, rR[k]);
+      rT[k] = fma(-lT, pk, rT[k]);
+    }
+    const double ph = shfl(ps ? hT : hR, src);
+    hR = fma(-lR, ph, hR);
+    hT = fma(-lT, ph, hT);
   }
-  const double ph = shfl(ps ? hT : hR, src);
-  hR = fma(-lR, ph, hR);
-  hT = fma(-lT, ph, hT);
 }
 
 template <int KC, int... Cs>
@@ -548,10 +559,13 @@ __device__ __forceinline__ void lu_solve_smem(const Geo& g, const WarpSmem& W, d
   for (int c = 0; c < N; ++c) {
     __syncwarp();
     const double vR = mR[c * 32], vT = mT[c * 32];
-    double piv;
-    int p;
-    lane_candidate(vR, vT, pR, pT, li, K, piv, p);
-    group_argmax<KB>(piv, p, g);
+    const unsigned kR = piv_key32(vR, li, pR), kT = piv_key32(vT, K + li, pT);
+    const unsigned km = group_max_u32<KB>(kR > kT ? kR : kT, g);
+    const int p = 127 - (int)(km & 127u);
+    // the pivot value from its owner's column (lanes outside every group
+    // read their own column)
+    const int own = g.valid ? g.base + (p >= K ? p - K : p) : g.lane;
+    const double piv = W.mat[(p >= K ? RS * 32 : 0) + c * 32 + own];
     ok = ok && (piv != 0.0) && cbcm::isfinite_(piv);
     const double rp = 1.0 / piv;
     const bool meR = (p == li), meT = (p == K + li);

@@ -136,14 +136,24 @@ struct Spec {
 // lu_solve_smem).  Unknowns x = (vr_0..vr_{K-1}, vt_0..vt_{K-1}); a holds N =
 // 2K rows of N + 1 entries (the right side last).  Gauss-Jordan elimination
 // with partial pivoting: for column c the pivot is the not-yet-pivot row with
-// the largest |a[r][c]| (NaN below every number, ties to the smaller row),
-// rp = 1 / pivot, the pivot row's entries k > c are read before the column's
+// the largest key (|a[r][c]| at 2^-13 relative resolution, NaN below every
+// number, ties to the smaller row), rp = 1 / pivot, the pivot row's entries k > c are read before the column's
 // updates, and every row r gets l = (r == p) ? 0 : a[r][c] * rp and
 // a[r][k] = fma(-l, pivot_row[k], a[r][k]) for k = c+1..N.  Then
 // x_c = a[p_c][N] * rp_c.  Returns false if a pivot is zero or not finite.
 bool lu_solve(int K, std::vector<double>& a, double* x) {
   const int N = 2 * K, RS = N + 1;
-  auto key = [](double v) { return v != v ? -1.0 : fabs(v); };
+  // pivot key: the high 32 bits of |a| with the low 7 bits replaced by
+  // 127 - row (magnitude at 2^-13 relative resolution, ties to the smaller
+  // row), NaN lowest (csrc/ckm1d_core.cuh, piv_key32)
+  auto key = [](double v, int r) {
+    uint64_t b;
+    memcpy(&b, &v, sizeof b);
+    b &= 0x7FFFFFFFFFFFFFFFull;
+    uint32_t hi = (uint32_t)(b >> 32);
+    if (b > 0x7FF0000000000000ull) hi = 0u;
+    return (hi & ~127u) | (uint32_t)(127 - r);
+  };
   bool pivoted[2 * KMAX] = {};
   int perm[2 * KMAX];
   double rps[2 * KMAX];
@@ -153,7 +163,7 @@ bool lu_solve(int K, std::vector<double>& a, double* x) {
     int p = -1;
     for (int r = 0; r < N; ++r) {
       if (pivoted[r]) continue;
-      if (p < 0 || key(a[(size_t)r * RS + c]) > key(a[(size_t)p * RS + c])) p = r;
+      if (p < 0 || key(a[(size_t)r * RS + c], r) > key(a[(size_t)p * RS + c], p)) p = r;
     }
     const double piv = a[(size_t)p * RS + c];
     ok = ok && (piv != 0.0) && cbcm::isfinite_(piv);
