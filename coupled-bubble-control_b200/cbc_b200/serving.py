@@ -120,6 +120,9 @@ class SolveServer:
         self.coup = RangeAllocator(coup)
         self.free_slots = deque(range(self.S))
         self.slot_K = np.zeros(self.S, np.int32)
+        # tick at which the slot's current request was admitted (-1: free);
+        # a read-back taken at an earlier tick says nothing about it
+        self.slot_tick = np.full(self.S, -1, np.int64)
         self.busy: Dict[int, Request] = {}
         self.busy_order = np.zeros(0, np.int32)     # occupied slots in admission order
         self.queue: deque = deque()
@@ -213,6 +216,7 @@ class SolveServer:
             r.slot, r.admitted = s, t
             r._ranges = (b, c)
             self.slot_K[s] = r.K
+            self.slot_tick[s] = self.ticks
             self.busy[s] = r
         self.busy_order = np.concatenate([self.busy_order, np.asarray([o[0] for o in offs], np.int32)])
         return n
@@ -262,16 +266,20 @@ class SolveServer:
             self.h_steps[par].copy_(self.d["steps"], non_blocking=True)
         ev = torch.cuda.Event()
         ev.record(self.stream)
-        self.readback[par] = (ev, self.busy_order.copy())
+        self.readback[par] = (ev, self.busy_order.copy(), self.ticks)
 
     def _harvest(self, par: int) -> int:
         """Releases the requests that had finished by the read-back `par`."""
         rb = self.readback[par]
         if rb is None:
             return 0
-        ev, slots = rb
+        ev, slots, tick = rb
         self.readback[par] = None
         ev.synchronize()
+        # only requests admitted no later than the read-back's tick and not
+        # released since (a slot may have been released by the other
+        # read-back and refilled after this one was taken)
+        slots = slots[(self.slot_tick[slots] >= 0) & (self.slot_tick[slots] <= tick)]
         if slots.size == 0:
             return 0
         st = self.h_status[par].numpy()
@@ -295,6 +303,7 @@ class SolveServer:
             b, c = r._ranges
             self.rows.free(b, r.K)
             self.coup.free(c, 3 * r.K * r.K)
+            self.slot_tick[s] = -1
             self.free_slots.append(int(s))
             self.completed.append(r)
         self.busy_order = self.busy_order[~np.isin(self.busy_order, done)]
