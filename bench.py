@@ -40,6 +40,15 @@ UNIT = "system-periods/s"
 MAX_STEPS = 1_000_000
 
 
+def status_counts_by_k(K, status):
+    """{K: {status: count}} of a finished solve."""
+    out = {}
+    for k in np.unique(K):
+        sel = np.asarray(K) == k
+        out[f"K{int(k)}"] = {int(a): int(b) for a, b in zip(*np.unique(np.asarray(status)[sel], return_counts=True))}
+    return out
+
+
 def lu_flops(K):
     """Flops of one direct solve (Gauss-Jordan with partial pivoting) of the
     N = 2K coupling system: N^2 (N + 1) multiply-adds (fma = 2) over every row
@@ -330,6 +339,7 @@ def lu_arm(scene, dev_index: int, schedule: str, flush, max_steps: int = MAX_STE
     out = {"value": adv / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
            "advanced_system_periods_per_step": adv,
            "status_counts": {int(k): int(v) for k, v in zip(*np.unique(res["status"], return_counts=True))},
+           "status_counts_by_K": status_counts_by_k(res["K"], res["status"]),
            "steps_per_solve": int(np.sum(res["steps"])), "algorithmic_gflop_per_step": flops / 1e9,
            "achieved_tflops": flops / (ms * 1e-3) / 1e12, "autotune": tune_info}
     if plain:
@@ -485,6 +495,7 @@ def run_b200(args):
     adv = float(np.sum(res["t"] - ens.host["t"]))
     flops = flop_count(res["K"], res["steps"], res["lin_iters"], args.lin_solver)
     status = {int(k): int(v) for k, v in zip(*np.unique(res["status"], return_counts=True))}
+    status_by_k = status_counts_by_k(res["K"], res["status"])
 
     total_ms_all, work_all = job_totals(total_ms, adv * args.steps, pg, dev)
     value = work_all / (total_ms_all * 1e-3)
@@ -547,7 +558,8 @@ def run_b200(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {**workload_config(args, world), "autotune": tune_info},
             "work": {"advanced_system_periods_per_step": adv, "nominal_system_periods": float(np.sum(scene.t_end)),
-                     "status_counts": status, "steps_per_solve": int(np.sum(res["steps"])),
+                     "status_counts": status, "status_counts_by_K": status_by_k,
+                     "steps_per_solve": int(np.sum(res["steps"])),
                      "richardson_sweeps_per_rhs": float(np.sum(res["lin_iters"]) / max(1, 6 * np.sum(res["steps"]))),
                      "algorithmic_gflop_per_step": flops / 1e9},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
