@@ -579,7 +579,7 @@ def run_b200(args):
         line["alone_latency"] = alone_latency(scene, local, "richardson")
         if args.served:
             line["served"] = {"offered_20k": served_measure(local, 20000.0, args.serve_seconds),
-                              "sustainable_1k": served_measure(local, 1000.0, args.serve_seconds)}
+                              "below_capacity_500": served_measure(local, 500.0, args.serve_seconds)}
         if args.large_k:
             line["large_k"] = large_k_measure(local, peak_tflops=peak)
         if lu:
@@ -630,7 +630,7 @@ def main():
     ap.add_argument("--no-cpu", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-env", dest="env", action="store_false")
     ap.add_argument("--no-served", dest="served", action="store_false",
-                    help="skip the served-stream measurement (Poisson 20k req/s and 1k req/s)")
+                    help="skip the served-stream measurement (Poisson 20k req/s and 500 req/s)")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--no-large-k", dest="large_k", action="store_false",
                     help="skip the large-K dense-output measurement")

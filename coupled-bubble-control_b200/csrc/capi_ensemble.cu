@@ -397,7 +397,24 @@ int32_t cbc_plan_launch(cbc_plan* p, void* stream) {
   if (!p) return fail(nullptr, CBC_E_INVALID, "plan is NULL");
   p->ctx->err.clear();
   DeviceGuard dg(p->ctx->device);
-  CBC_CUDA_TRY(p->ctx, cudaGraphLaunch(p->exec, (cudaStream_t)stream));
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CBC_CUDA_TRY(p->ctx, cudaStreamIsCapturing(st, &cap));
+  if (cap == cudaStreamCaptureStatusActive) {
+    // the caller is capturing its own graph (e.g. torch.cuda.graph): a graph
+    // launch is not allowed there, so the plan's graph becomes a child node
+    // of the graph being captured, after the stream's current dependencies
+    cudaGraph_t outer = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    unsigned long long id = 0;
+    CBC_CUDA_TRY(p->ctx, cudaStreamGetCaptureInfo(st, &cap, &id, &outer, &deps, &ndeps));
+    cudaGraphNode_t node = nullptr;
+    CBC_CUDA_TRY(p->ctx, cudaGraphAddChildGraphNode(&node, outer, deps, ndeps, p->graph));
+    CBC_CUDA_TRY(p->ctx, cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  } else {
+    CBC_CUDA_TRY(p->ctx, cudaGraphLaunch(p->exec, st));
+  }
   p->ctx->launches += p->kernels;
   return CBC_OK;
 }

@@ -296,7 +296,10 @@ int32_t cbc_ensemble_solve_noalloc(cbc_context* ctx, const cbc_spec* spec, const
                                    const cbc_work* work, int64_t max_steps, void* stream);
 
 /* Captures the same launch sequence into a CUDA graph bound to these buffers;
- * cbc_plan_launch replays it on `stream` (one graph launch per solve). */
+ * cbc_plan_launch replays it on `stream` (one graph launch per solve).  If
+ * `stream` is itself being captured into a graph of the caller's (e.g. by
+ * torch.cuda.graph), cbc_plan_launch adds the plan's graph as a child node of
+ * that graph instead of launching it. */
 int32_t cbc_plan_create(cbc_context* ctx, const cbc_spec* spec, const cbc_ensemble* ens,
                         const cbc_work* work, int64_t max_steps, cbc_plan** out);
 int32_t cbc_plan_launch(cbc_plan* plan, void* stream);
