@@ -36,6 +36,8 @@ for _p in (os.path.join(ROOT, "coupled-bubble-control_b200"), ROOT):
 import numpy as np  # noqa: E402
 
 METRIC = "system-periods/s @rtol 1e-9, batched vs plain; p50/p99 env-step latency"
+# DRAM traffic of the dominant kernel per launch (ncu, see roofline.traffic_note)
+TRAFFIC_K8_BYTES = 20103680
 UNIT = "system-periods/s"
 MAX_STEPS = 1_000_000
 
@@ -563,7 +565,12 @@ def run_b200(args):
                      "richardson_sweeps_per_rhs": float(np.sum(res["lin_iters"]) / max(1, 6 * np.sum(res["steps"]))),
                      "algorithmic_gflop_per_step": flops / 1e9},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": TRAFFIC_K8_BYTES,
+                         "traffic_note": "DRAM bytes (read + write) of one ensemble_kernel<8,8> launch over the "
+                                         "K = 8 bucket filling the GPU, ncu capture in profiles/"
+                                         "ensemble_kernel_k8_richardson_steady_state.md: the state, parameters "
+                                         "and coupling are read once per launch and stay on chip; traffic does "
+                                         "not grow with the steps taken",
                          "note": "algorithmic FP64 flops (transcendentals counted as 1) / graph time; "
                                  "peak = cuBLAS FP64 GEMM measured in this run"},
             "clocks": clk.summary(),
