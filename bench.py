@@ -256,6 +256,37 @@ def batched_once(scene, dev_index: int, schedule: str) -> float:
     return adv / dt
 
 
+def plain_study_measure(dev_index: int, cpu_systems: int = 64):
+    """The plain parameter study (1,024 systems of K = 2, 10 periods, 32
+    samples per period, seed 0) through the reference drop-in path
+    (Model.solve: reference-layout buffers, relaunch every 2,048 steps with a
+    host completion check), and the CPU oracle on `cpu_systems` of them on
+    every host core."""
+    import torch
+    from cbc_b200 import scenes
+    from oracle import oracle
+    sc = scenes.plain_study(ns=1024, periods=10.0, samples_per_period=32, seed=0)
+    m = scenes.build_model(sc)
+    m._ensure_buffers()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    m.solve(max_steps=MAX_STEPS, kernel_steps=2048)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    adv = float(m.runtime.device_buffers.state.actual_time.sum().item())
+    sub = scenes.subset(sc, np.arange(cpu_systems))
+    mc = scenes.build_model(sub)
+    t1 = time.perf_counter()
+    buf = oracle.solve_model(mc, max_steps=MAX_STEPS, kernel_steps=2048)
+    cdt = time.perf_counter() - t1
+    cadv = float(np.sum(buf["actual_time"]))
+    return {"workload": "plain_study_1024xK2_10periods_321samples", "value": adv / dt, "unit": UNIT,
+            "seconds": dt, "path": "Model.solve (reference layout, relaunch every 2048 steps)",
+            "cpu_oracle": {"value": cadv / cdt, "unit": UNIT, "systems": cpu_systems,
+                           "cores": os.cpu_count() or 1},
+            "gpu_vs_cpu": (adv / dt) / (cadv / cdt)}
+
+
 def plain_per_k(scene, dev, solver_spec=None):
     """The reference execution model on the same systems: one reference-layout
     solve per K (cbc_solve, relaunch every 2048 steps with a host check)."""
@@ -505,7 +536,9 @@ def run_b200(args):
     # end-to-end through the public API from host buffers (rank-local)
     e2e = None
     if args.e2e:
-        keys_in = ("state", "t", "h", "event", "status", "steps", "rejected", "conv_ok", "conv_fail", "lin_iters")
+        # every input array of the ensemble goes up each step (state, offsets,
+        # bubble / system / control parameters, coupling, times, counters)
+        keys_in = tuple(k for k in ens.host if k != "K")
         keys_out = ("state", "t", "h", "event", "status", "steps", "rejected", "conv_ok", "conv_fail", "lin_iters")
         pin_in = {k: torch.from_numpy(np.ascontiguousarray(ens.host[k])).pin_memory() for k in keys_in}
         pin_out = {k: torch.empty_like(ens.dev[k], device="cpu").pin_memory() for k in keys_out}
@@ -589,6 +622,8 @@ def run_b200(args):
                               "below_capacity_500": served_measure(local, 500.0, args.serve_seconds)}
         if args.large_k:
             line["large_k"] = large_k_measure(local, peak_tflops=peak)
+        if args.plain_study:
+            line["plain_study"] = plain_study_measure(local)
         if lu:
             lu["roofline_frac"] = lu["achieved_tflops"] / peak
             line["lin_solver_lu"] = lu
@@ -639,6 +674,8 @@ def main():
     ap.add_argument("--no-served", dest="served", action="store_false",
                     help="skip the served-stream measurement (Poisson 20k req/s and 500 req/s)")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--no-plain-study", dest="plain_study", action="store_false",
+                    help="skip the plain parameter study (1,024 x K = 2, 10 periods) through Model.solve")
     ap.add_argument("--no-large-k", dest="large_k", action="store_false",
                     help="skip the large-K dense-output measurement")
     ap.add_argument("--workload", default="mixed_k", choices=["mixed_k", "alone"],
