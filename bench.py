@@ -168,34 +168,45 @@ def measured_fp64_peak(dev) -> float:
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_baseline(scene, seconds: float = 12.0, nthreads: int = 0, seed: int = 99):
+def cpu_baseline(scene, seconds: float = 12.0, nthreads: int = 0, seed: int = 99, step_cap: int = 300_000):
     """The CPU oracle (C++ restatement of the reference integrator, all host
-    cores) on a bounded random sample of the same workload: batches of 64
-    systems (spans capped at 5 periods) until `seconds` of CPU time are spent."""
+    cores) on a bounded random sample of the same workload: batches of
+    systems drawn at random, each integrated over its FULL span (at most
+    `step_cap` steps), until `seconds` of wall time are spent.  The K groups
+    of a batch run concurrently (host threads split among them by size), so
+    every core stays busy.  Counts the system-periods advanced."""
+    from concurrent.futures import ThreadPoolExecutor
     from cbc_b200 import scenes
     from oracle import oracle
+    cores = nthreads if nthreads > 0 else (os.cpu_count() or 1)
     rng = np.random.default_rng(seed)
     perm = rng.permutation(scene.ns)
-    cap = 5.0
-    total_adv, n_done, pos = 0.0, 0, 0
+    batch = 8 * cores
+    total_adv, n_done, pos, capped = 0.0, 0, 0, 0
     t0 = time.perf_counter()
+
+    def run(sub, threads):
+        m = scenes.build_model(sub, ndo=0)
+        return oracle.solve_model(m, max_steps=step_cap, kernel_steps=step_cap, nthreads=threads)
+
     while time.perf_counter() - t0 < seconds and pos < scene.ns:
-        idx = np.sort(perm[pos:pos + 64])
-        pos += 64
+        idx = np.sort(perm[pos:pos + batch])
+        pos += batch
         sub = scenes.subset(scene, idx)
-        sub.t_end = np.minimum(sub.t_end, cap)
-        for k in np.unique(sub.K):
-            sel = np.nonzero(sub.K == k)[0]
-            m = scenes.build_model(scenes.subset(sub, sel), ndo=0)
-            buf = oracle.solve_model(m, max_steps=MAX_STEPS, kernel_steps=MAX_STEPS, nthreads=nthreads)
-            total_adv += float(np.sum(buf["actual_time"]))
+        groups = [np.nonzero(sub.K == k)[0] for k in np.unique(sub.K)]
+        with ThreadPoolExecutor(len(groups)) as ex:
+            futs = [ex.submit(run, scenes.subset(sub, g), max(1, round(cores * g.size / idx.size))) for g in groups]
+            for f in futs:
+                buf = f.result()
+                total_adv += float(np.sum(buf["actual_time"]))
+                capped += int(np.sum(buf["status_flags"] == -1))
         n_done += idx.size
     dt = time.perf_counter() - t0
-    cores = nthreads if nthreads > 0 else (os.cpu_count() or 1)
     return {"value": total_adv / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n_done} systems drawn at random from the same mixed-K ensemble, spans capped at "
-                      f"{cap} periods ({total_adv:.1f} system-periods in {dt:.1f} s), CPU oracle "
-                      f"(C++ restatement of the reference integrator) on {cores} threads"}
+            "sample": f"{n_done} systems drawn at random from the same mixed-K ensemble, each over its full "
+                      f"5-50 period span ({capped} stopped at the {step_cap}-step cap), {total_adv:.1f} "
+                      f"system-periods in {dt:.1f} s, CPU oracle (C++ restatement of the reference "
+                      f"integrator) on {cores} threads"}
 
 
 def workload_config(args, world: int) -> dict:
