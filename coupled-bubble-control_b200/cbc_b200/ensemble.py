@@ -363,10 +363,10 @@ class Ensemble:
         return Plan(self, max_steps, work)
 
     def adaptive_plan(self, max_steps: int = 1_000_000, slices=(1.0, 2.0, 4.0, 8.0),
-                      max_lane_sms: int = 32, load_factor: float = 1.45) -> "AdaptivePlan":
+                      max_lane_sms: int = 32, load_factor: float = 1.45, solo: int = 0) -> "AdaptivePlan":
         if not self.dev:
             self.to_device()
-        return AdaptivePlan(self, max_steps, slices, max_lane_sms, load_factor)
+        return AdaptivePlan(self, max_steps, slices, max_lane_sms, load_factor, solo)
 
     def scheduled_plan(self, max_steps: int = 1_000_000, pilot_steps: int = 2048,
                        latency_lane: bool = True) -> "ScheduledPlan":
@@ -443,11 +443,16 @@ class ScheduledPlan:
 
 
 def lane_work_list(wl: WorkList, K: np.ndarray, lane_ids: np.ndarray, order_key: np.ndarray,
-                   sms_by_k: Dict[int, int]) -> WorkList:
+                   sms_by_k: Dict[int, int], solo_ids=()) -> WorkList:
     """Moves the systems lane_ids out of the buckets of wl into latency lanes:
     one extra bucket per K with sms_by_k[K] exclusive SMs, longest order_key
-    first."""
+    first.  Systems in solo_ids (a subset of lane_ids) get solo lanes: a
+    bucket of their K whose warps hold one system each (slots = 1), so their
+    Richardson loop never waits for warp-mates; four per exclusive SM."""
     lane_ids = np.asarray(lane_ids)
+    solo_ids = np.asarray(solo_ids, dtype=np.int64)
+    if solo_ids.size:
+        lane_ids = lane_ids[~np.isin(lane_ids, solo_ids)]
     order, bk, bb = [], [], [0]
     share = [] if wl.share is not None else None
     excl = []
@@ -471,14 +476,26 @@ def lane_work_list(wl: WorkList, K: np.ndarray, lane_ids: np.ndarray, order_key:
         excl.append(int(sms_by_k[k]))
         if share is not None:
             share.append(0.0)
+    slots = [32 // int(k) for k in bk]
+    for k in sorted(set(int(x) for x in K[solo_ids])) if solo_ids.size else []:
+        sel = solo_ids[K[solo_ids] == k]
+        sel = sel[np.argsort(-order_key[sel], kind="stable")]
+        order.append(sel.astype(np.int32))
+        bk.append(int(k))
+        bb.append(bb[-1] + sel.size)
+        excl.append(int((sel.size + 3) // 4))
+        slots.append(1)
+        if share is not None:
+            share.append(0.0)
     return WorkList(order=np.concatenate(order).astype(np.int32), bucket_K=np.asarray(bk, np.int32),
                     bucket_begin=np.asarray(bb, np.int32),
                     share=None if share is None else np.asarray(share, np.float32),
-                    exclusive=np.asarray(excl, np.int32))
+                    exclusive=np.asarray(excl, np.int32),
+                    slots=np.asarray(slots, np.int32) if solo_ids.size else None)
 
 
 def adaptive_work_list(K, t_end, t0, a0, t, attempts, active, sm_count: int, max_lane_sms: int = 32,
-                       load_factor: float = 1.45, min_observed: int = 256):
+                       load_factor: float = 1.45, min_observed: int = 256, solo: int = 0):
     """One re-planning step of ``AdaptivePlan`` (host only): the work list
     for the systems still running, from the progress since the solve began
     (t0 / a0: simulated time and step attempts then; t / attempts: now).
@@ -516,9 +533,11 @@ def adaptive_work_list(K, t_end, t0, a0, t, attempts, active, sm_count: int, max
             lane_sms += 1
         count[k] = count.get(k, 0) + 1
         picked.append(int(s))
+    solo_ids = np.asarray(picked[:solo], dtype=np.int64)    # the longest chains run alone in their warp
     if picked:
-        wl = lane_work_list(wl, K, np.asarray(picked), serial_s, sms)
+        wl = lane_work_list(wl, K, np.asarray(picked), serial_s, sms, solo_ids=solo_ids)
     info = {"active": int(ids.size), "bulk_s": bulk_s, "lane_systems": len(picked), "lane_sms": lane_sms,
+            "solo_systems": int(solo_ids.size),
             "max_serial_s": float(serial_s[ids].max()) if ids.size else 0.0}
     return wl, info
 
@@ -554,19 +573,20 @@ class AdaptivePlan:
     MIN_OBSERVED = 256   # attempts before a system's own rate is trusted
 
     def __init__(self, ens: Ensemble, max_steps: int, slices=(1.0, 2.0, 4.0, 8.0), max_lane_sms: int = 32,
-                 load_factor: float = 1.45):
+                 load_factor: float = 1.45, solo: int = 0):
         self.ens = ens
         self.max_steps = int(max_steps)
         self.slices = [float(s) for s in slices]
         self.max_lane_sms = int(max_lane_sms)
         self.load_factor = float(load_factor)
+        self.solo = int(solo)
         self.history: List[dict] = []
         import torch
         self.sm_count = torch.cuda.get_device_properties(ens.device).multi_processor_count
 
     def plan(self, K, t_end, t0, a0, t, attempts, active) -> WorkList:
         wl, info = adaptive_work_list(K, t_end, t0, a0, t, attempts, active, self.sm_count, self.max_lane_sms,
-                                      self.load_factor, self.MIN_OBSERVED)
+                                      self.load_factor, self.MIN_OBSERVED, self.solo)
         self.history.append(info)
         return wl
 
