@@ -451,14 +451,16 @@ def lane_work_list(wl: WorkList, K: np.ndarray, lane_ids: np.ndarray, order_key:
     Richardson loop never waits for warp-mates; four per exclusive SM."""
     lane_ids = np.asarray(lane_ids)
     solo_ids = np.asarray(solo_ids, dtype=np.int64)
+    moved = lane_ids                        # every system leaving the ordinary buckets
     if solo_ids.size:
+        moved = np.union1d(lane_ids, solo_ids)
         lane_ids = lane_ids[~np.isin(lane_ids, solo_ids)]
     order, bk, bb = [], [], [0]
     share = [] if wl.share is not None else None
     excl = []
     for b in range(wl.bucket_K.size):
         seg = wl.order[wl.bucket_begin[b]:wl.bucket_begin[b + 1]]
-        seg = seg[~np.isin(seg, lane_ids)]
+        seg = seg[~np.isin(seg, moved)]
         order.append(seg)
         bk.append(int(wl.bucket_K[b]))
         bb.append(bb[-1] + seg.size)

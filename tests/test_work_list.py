@@ -55,3 +55,29 @@ def test_adaptive_replanning_host_logic():
     # inside the default lane budget of 32 SMs
     wl2, info2 = adaptive_work_list(K, np.full(n, 0.01), t0, a0, t0, a0, active, sm_count=148)
     assert sorted(wl2.order.tolist()) == sorted(np.nonzero(active)[0].tolist()) and info2["lane_sms"] <= 32
+
+
+def test_solo_lanes_keep_every_system_once():
+    """Solo lanes (one system per warp) for the longest chains: every active
+    system appears exactly once in the work list, solo buckets hold one
+    system per warp and four per exclusive SM."""
+    from cbc_b200.ensemble import adaptive_work_list
+    rng = np.random.default_rng(5)
+    n = 3000
+    K = rng.choice([2, 3, 4, 8], size=n)
+    t_end = rng.uniform(5.0, 50.0, size=n)
+    t0 = np.zeros(n)
+    a0 = np.zeros(n, np.int64)
+    t = rng.uniform(0.0, 1.0, size=n)
+    attempts = (t * rng.uniform(500, 20000, size=n)).astype(np.int64) + 300
+    active = np.ones(n, bool)
+    for solo in (0, 3, 8):
+        wl, info = adaptive_work_list(K, t_end, t0, a0, t, attempts, active, 148, max_lane_sms=16, solo=solo)
+        assert sorted(wl.order.tolist()) == list(range(n))
+        assert info["solo_systems"] == min(solo, info["lane_systems"])
+        if solo and info["solo_systems"]:
+            solo_b = [b for b in range(wl.bucket_K.size) if wl.slots is not None and wl.slots[b] == 1]
+            assert solo_b
+            for b in solo_b:
+                seg = wl.order[wl.bucket_begin[b]:wl.bucket_begin[b + 1]]
+                assert wl.exclusive[b] == (seg.size + 3) // 4 and np.all(K[seg] == wl.bucket_K[b])
