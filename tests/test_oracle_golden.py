@@ -28,6 +28,12 @@ controller's error estimate is a small difference of stage values), which
 moves mid-run samples by ~1e-9 relative while end states, where both land
 exactly on t_end, agree to 1e-16.
 
+The collapse case (golden_ref_numba_collapse.npz: two bubbles, 0.9 periods,
+1,650 steps; bubble 0 grows to R = 3.6, collapses to R ~ 0.18 and rebounds)
+agrees at the end to 2.3e-13 relative and sample by sample to 2.1e-7 on
+dR/dt, 1.1e-8 on R (sample-time drift 1.9e-9 relative, while dR/dt changes
+by orders of magnitude between steps); its dense bound is 5e-7.
+
 Cases that end on a collision event (status 2) stop at the first accepted
 step whose collision gap is below ETOL, so their end time depends on the
 exact step grid.  The controller's step sizes follow the embedded error
@@ -86,7 +92,11 @@ def test_oracle_matches_reference_numba(name, z):
         da = buf["dense_state"][:n, :, :, :K]
         db = final["dense_state"][:n, :, :, :K]
         derr = np.abs(da - db) / np.maximum(np.abs(db), 1e-12)
-        assert np.max(derr) < 1e-7, f"max relative dense-sample error {np.max(derr):.3e}"
+        # through a collapse dR/dt changes by orders of magnitude between
+        # steps, so the ~2e-9 relative drift of the sample times moves dR/dt
+        # samples by up to ~2e-7 while the end state agrees to 2e-13
+        dbound = 5e-7 if "collapse" in name else 1e-7
+        assert np.max(derr) < dbound, f"max relative dense-sample error {np.max(derr):.3e}"
     assert np.all(buf["status_flags"] == final["status_flags"]), (buf["status_flags"], final["status_flags"])
     event_end = bool(np.all(final["status_flags"] == 2))
     np.testing.assert_allclose(buf["actual_time"], final["actual_time"], rtol=1e-8 if event_end else 0,
