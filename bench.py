@@ -689,8 +689,10 @@ def main():
                     help="skip the plain parameter study (1,024 x K = 2, 10 periods) through Model.solve")
     ap.add_argument("--no-large-k", dest="large_k", action="store_false",
                     help="skip the large-K dense-output measurement")
-    ap.add_argument("--workload", default="mixed_k", choices=["mixed_k", "alone"],
-                    help="alone: only the single-system step latency of both coupling solvers")
+    ap.add_argument("--workload", default="mixed_k", choices=["mixed_k", "alone", "large_k"],
+                    help="alone: only the single-system step latency of both coupling solvers; large_k: only "
+                         "the large-K dense-output measurement (--ns systems of K = 32, --periods)")
+    ap.add_argument("--periods", type=float, default=0.5, help="span of the large_k workload")
     ap.add_argument("--lin-solver", default="richardson", choices=["richardson", "lu"],
                     help="implicit-coupling solver of the headline arm (richardson: the reference's)")
     ap.add_argument("--only-k", type=int, default=0,
@@ -711,6 +713,12 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.workload == "alone":
         run_alone(args)
+    elif args.workload == "large_k":
+        import torch
+        torch.cuda.set_device(0)
+        line = large_k_measure(0, ns=args.ns, periods=args.periods)
+        line.update({"metric": METRIC, "n_gpus": 1, "dtype": "f64", "data": "synthetic"})
+        print(json.dumps(line), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     else:
