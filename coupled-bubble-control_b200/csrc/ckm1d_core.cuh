@@ -187,14 +187,8 @@ __host__ __device__ inline int pv_doubles(int K, int lin) {
   return (K > 8 && lin == LIN_LU) ? (((32 / K) * (2 * K + 1) + 1) & ~1) : 0;
 }
 
-// Staged coupling coefficients M(c, j, i) of each lane's partners: K <= 8
-// only.  For K > 8 they are read from the coupling array in global memory
-// (cached) at each use, which frees 3 (K - 1) 32 doubles per warp (24 KB at
-// K = 32) of shared memory for more resident warps.
-__host__ __device__ inline int cm_doubles(int K) { return K <= 8 ? 3 * (K - 1) * 32 : 0; }
-
 __host__ __device__ inline int smem_doubles_per_warp(int K, int nk, int lin = LIN_RICHARDSON) {
-  return hc_doubles(K, nk) + NUPS * 32 + 24 * 32 + XV_DOUBLES + cm_doubles(K) + mat_doubles(K, lin) +
+  return hc_doubles(K, nk) + NUPS * 32 + 24 * 32 + XV_DOUBLES + 3 * (K - 1) * 32 + mat_doubles(K, lin) +
          pv_doubles(K, lin);
 }
 
@@ -206,7 +200,7 @@ __device__ __forceinline__ WarpSmem warp_smem(double* base, int K, int nk, int l
   w.ks = w.up + NUPS * 32;
   w.xv = w.ks + 24 * 32;
   w.cm = w.xv + XV_DOUBLES;
-  w.mat = w.cm + cm_doubles(K);
+  w.mat = w.cm + 3 * (K - 1) * 32;
   w.pv = w.mat + mat_doubles(K, lin);
   return w;
 }
@@ -221,7 +215,6 @@ struct MView {
 // j = (i + d) mod K, d = 1..K-1, into shared memory: they are constant for the
 // whole solve and are read every RHS evaluation.
 __device__ __forceinline__ void store_coupling(const WarpSmem& w, const Geo& g, const MView& M) {
-  if (g.K > 8) return;   // read from global memory at each use (cm_doubles)
   for (int d = 1; d < g.K; ++d) {
     const int j = partner_lane(g, d) - g.base;
 #pragma unroll
@@ -229,14 +222,8 @@ __device__ __forceinline__ void store_coupling(const WarpSmem& w, const Geo& g, 
   }
 }
 
-template <int KB>
-__device__ __forceinline__ double cmv(const WarpSmem& w, const Geo& g, const MView& M, int c, int d) {
-  if constexpr (KB <= 8) {
-    return w.cm[(c * (g.K - 1) + d - 1) * 32 + g.lane];
-  } else {
-    const int j = partner_lane(g, d) - g.base;
-    return __ldg(M.m + c * M.sc + j * M.sj);
-  }
+__device__ __forceinline__ double cmv(const WarpSmem& w, const Geo& g, int c, int d) {
+  return w.cm[(c * (g.K - 1) + d - 1) * 32 + g.lane];
 }
 
 // Per-lane integrator state (bubble + copies of the system scalars).
@@ -715,9 +702,9 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
         const double rd2 = rd * rd;
         const double srd2 = rd2 * sg;
         const double rd3 = rd2 * rd;
-        const double m0 = cmv<KB>(W, g, M, 0, d);
-        const double m1 = cmv<KB>(W, g, M, 1, d);
-        const double m2 = cmv<KB>(W, g, M, 2, d);
+        const double m0 = cmv(W, g, 0, d);
+        const double m1 = cmv(W, g, 1, d);
+        const double m2 = cmv(W, g, 2, d);
         double t0 = fma(2.5 * srd2, h2j, rd3 * h4j);
         t0 = fma(2.0 * rd, h0j, t0);
         g0 = fma(-m0, t0, g0);
