@@ -679,11 +679,7 @@ def run_alone(args):
         u = scenes.uniform(k, ns=4, periods=3.0, seed=90 + k, pa_hi=1.2 if k > 8 else 1.5,
                            x_range=(-0.5, 0.5) if k > 8 else (-0.25, 0.25))
         extra.append(u)
-    sc = mix
-    for u in extra:
-        sc = scenes.Scene(K=np.concatenate([sc.K, u.K]), R0=sc.R0 + u.R0, PA=np.hstack([sc.PA, u.PA]),
-                          FR=np.hstack([sc.FR, u.FR]), PS=np.hstack([sc.PS, u.PS]), X0=sc.X0 + u.X0,
-                          t_end=np.concatenate([sc.t_end, u.t_end]), ac="SW_A")
+    sc = scenes.concat(mix, *extra)
     ks = (1, 2, 3, 4, 5, 6, 7, 8, 16, 32)
     out = {"workload": "alone_latency", "unit": "us per step attempt",
            "richardson": alone_latency(sc, 0, "richardson", ks=ks), "lu": alone_latency(sc, 0, "lu", ks=ks)}
@@ -708,9 +704,10 @@ def main():
                     help="skip the plain parameter study (1,024 x K = 2, 10 periods) through Model.solve")
     ap.add_argument("--no-large-k", dest="large_k", action="store_false",
                     help="skip the large-K dense-output measurement")
-    ap.add_argument("--workload", default="mixed_k", choices=["mixed_k", "alone", "large_k"],
+    ap.add_argument("--workload", default="mixed_k", choices=["mixed_k", "alone", "large_k", "served"],
                     help="alone: only the single-system step latency of both coupling solvers; large_k: only "
-                         "the large-K dense-output measurement (--ns systems of K = 32, --periods)")
+                         "the large-K dense-output measurement (--ns systems of K = 32, --periods); served: "
+                         "only the served streams (20k and 500 req/s, --serve-seconds)")
     ap.add_argument("--periods", type=float, default=0.5, help="span of the large_k workload")
     ap.add_argument("--lin-solver", default="richardson", choices=["richardson", "lu"],
                     help="implicit-coupling solver of the headline arm (richardson: the reference's)")
@@ -737,6 +734,13 @@ def main():
         torch.cuda.set_device(0)
         line = large_k_measure(0, ns=args.ns, periods=args.periods)
         line.update({"metric": METRIC, "n_gpus": 1, "dtype": "f64", "data": "synthetic"})
+        print(json.dumps(line), flush=True)
+    elif args.workload == "served":
+        import torch
+        torch.cuda.set_device(0)
+        line = {"workload": "served", "metric": METRIC, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+                "offered_20k": served_measure(0, 20000.0, args.serve_seconds),
+                "below_capacity_500": served_measure(0, 500.0, args.serve_seconds)}
         print(json.dumps(line), flush=True)
     elif args.impl == "reference":
         run_reference(args)

@@ -153,6 +153,19 @@ def subset(scene: Scene, idx) -> Scene:
                  ndo=scene.ndo, name=scene.name, meta=dict(scene.meta))
 
 
+def concat(*parts: Scene) -> Scene:
+    """One scene holding the systems of `parts` in order (same field type)."""
+    if not parts:
+        raise ValueError("nothing to concatenate")
+    if len({p.ac for p in parts}) != 1 or len({p.nk for p in parts}) != 1:
+        raise ValueError("scenes differ in field type or harmonics count")
+    return Scene(K=np.concatenate([p.K for p in parts]), R0=[r for p in parts for r in p.R0],
+                 PA=np.hstack([p.PA for p in parts]), FR=np.hstack([p.FR for p in parts]),
+                 PS=np.hstack([p.PS for p in parts]), X0=[x for p in parts for x in p.X0],
+                 t_end=np.concatenate([p.t_end for p in parts]), ac=parts[0].ac, ndo=max(p.ndo for p in parts),
+                 name="+".join(p.name for p in parts if p.name))
+
+
 def build_model(scene: Scene, solver_spec=None, backend=None, ndo: Optional[int] = None):
     """A ``CKM1D`` model (uniform K) whose host buffers hold the scene.
 

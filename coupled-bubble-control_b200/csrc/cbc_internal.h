@@ -182,6 +182,8 @@ decltype(auto) dispatch_k(int K, F&& f) {
     case 6: return f(IC<8>{}, IC<6>{});
     case 7: return f(IC<8>{}, IC<7>{});
     case 8: return f(IC<8>{}, IC<8>{});
+    case 16: return f(IC<16>{}, IC<16>{});
+    case 32: return f(IC<32>{}, IC<32>{});
     default:
       if (K <= 16) return f(IC<16>{}, IC<0>{});
       return f(IC<32>{}, IC<0>{});

@@ -174,8 +174,9 @@ __host__ __device__ inline int hc_doubles(int K, int nk) { return (HC_PER_K * nk
 
 // Matrix region per warp:
 //   Richardson, K <= 8: none (the partner coefficients live in registers);
-//   Richardson, K > 8:  the four partner-coefficient arrays [4][K-1][32]
-//                       (kept out of registers: local memory would spill to L2);
+//   Richardson, K > 8:  the partner coefficients as double2 records
+//                       [K-1][(A,B), (C,D)][32] (kept out of registers: local
+//                       memory would spill to L2);
 //   direct, K <= 8:     staging of the four coefficient blocks by absolute
 //                       column, [4][K][32], read back into register rows;
 //   direct, K > 8:      the two augmented rows of every lane, [2][2K+1][32].
@@ -375,23 +376,29 @@ __device__ __forceinline__ void residual(const Geo& g, const double* Am, const d
   r1 = b1 - (st + vt);
 }
 
-// The same with the coefficients in shared memory: m[(q (K-1) + d - 1) 32]
-// for q = 0..3 (A, B, C, D), m pointing at this lane's column.
+// The same for K > 8, from shared memory: the coefficients of partner
+// distance d as two double2 records per lane, (A, B) at [(d - 1) 2][lane] and
+// (C, D) at [(d - 1) 2 + 1][lane]; the partner iterates through the warp's
+// exchange records (one 16-byte store per lane and one 16-byte load per
+// partner, instead of two 64-bit shuffles per partner).  Same values and the
+// same accumulation order as the register form.
 template <int KB>
-__device__ __forceinline__ void residual_smem(const Geo& g, const double* m, double cpf0, double b0, double b1,
+__device__ __forceinline__ void residual_smem(const Geo& g, const WarpSmem& W, double cpf0, double b0, double b1,
                                               double vr, double vt, double& r0, double& r1) {
   double ar[4] = {0.0, 0.0, 0.0, 0.0}, at[4] = {0.0, 0.0, 0.0, 0.0};
-  const int K1 = g.K - 1;
+  const double2* m2 = reinterpret_cast<const double2*>(W.mat) + g.lane;
+  double2* xr = reinterpret_cast<double2*>(W.xv);
+  __syncwarp();
+  xr[g.lane] = make_double2(vr, vt);
+  __syncwarp();
 #pragma unroll
   for (int d = 1; d < KB; ++d)
     if (d < g.K) {
-      const int src = partner_lane(g, d);
-      const double vrj = shfl(vr, src), vtj = shfl(vt, src);
+      const double2 vj = xr[partner_rec(g, d)];
       const int c = (d - 1) & 3;
-      const double A = m[(0 * K1 + d - 1) * 32], B = m[(1 * K1 + d - 1) * 32];
-      const double C = m[(2 * K1 + d - 1) * 32], D = m[(3 * K1 + d - 1) * 32];
-      ar[c] = fma(A, vrj, fma(B, vtj, ar[c]));
-      at[c] = fma(C, vrj, fma(D, vtj, at[c]));
+      const double2 ab = m2[(2 * (d - 1)) * 32], cd = m2[(2 * (d - 1) + 1) * 32];
+      ar[c] = fma(ab.x, vj.x, fma(ab.y, vj.y, ar[c]));
+      at[c] = fma(cd.x, vj.x, fma(cd.y, vj.y, at[c]));
     }
   const int nc = g.K - 1 < 4 ? g.K - 1 : 4;
   const double sr = tree_open(ar, nc);
@@ -663,7 +670,6 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
   double g0 = 0.0, g1 = 0.0, tn = 0.0, tg2 = 0.0, tg3 = 0.0;
   double Am[REG ? KB : 1], Bm[REG ? KB : 1], Cm[REG ? KB : 1], Dm[REG ? KB : 1];
   double* mcol = W.mat + g.lane;
-  const int K1 = K - 1;
   const int RS = 2 * K + 1;
   // partner states through the exchange records
   double2* xv2 = reinterpret_cast<double2*>(W.xv);
@@ -724,10 +730,9 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
           Cm[d] = c_;
           Dm[d] = d_;
         } else if constexpr (LIN == LIN_RICHARDSON) {
-          mcol[(0 * K1 + d - 1) * 32] = a_;
-          mcol[(1 * K1 + d - 1) * 32] = b_;
-          mcol[(2 * K1 + d - 1) * 32] = c_;
-          mcol[(3 * K1 + d - 1) * 32] = d_;
+          double2* mcol2 = reinterpret_cast<double2*>(W.mat) + g.lane;
+          mcol2[(2 * (d - 1)) * 32] = make_double2(a_, b_);
+          mcol2[(2 * (d - 1) + 1) * 32] = make_double2(c_, d_);
         } else {
           const int j = partner_lane(g, d) - g.base;   // absolute partner column
           if constexpr (KB <= 8) {
@@ -821,7 +826,7 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
   const bool full_groups = (g.K == KB);
   double r0, r1;
   if constexpr (REG) residual<KB>(g, Am, Bm, Cm, Dm, cpf0, b0, b1, vr, vt, r0, r1);
-  else residual_smem<KB>(g, mcol, cpf0, b0, b1, vr, vt, r0, r1);
+  else residual_smem<KB>(g, W, cpf0, b0, b1, vr, vt, r0, r1);
   for (int it = 0; it < P.lin_max_iter; ++it) {
     if (__all_sync(FULL, found)) break;
     const double rr = fma(r0, r0, r1 * r1);
@@ -836,7 +841,7 @@ __device__ __forceinline__ void rhs(const Geo& g, const Params& P, const WarpSme
     vr = fma(P.omega, r0, vr);
     vt = fma(P.omega, r1, vt);
     if constexpr (REG) residual<KB>(g, Am, Bm, Cm, Dm, cpf0, b0, b1, vr, vt, r0, r1);
-    else residual_smem<KB>(g, mcol, cpf0, b0, b1, vr, vt, r0, r1);
+    else residual_smem<KB>(g, W, cpf0, b0, b1, vr, vt, r0, r1);
   }
   conv = found;
   if (found) {

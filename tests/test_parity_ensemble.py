@@ -72,6 +72,23 @@ def test_mixed_k_bit_exact(cuda, use_graph):
     assert np.all(gpu["status"] != 0)
 
 
+def test_large_k_buckets_bit_exact(cuda):
+    """Buckets of K = 12, 16, 24, 32 in one ensemble: kernels compiled for
+    the exact K (16, 32) and for a run-time K (12, 24)."""
+    import torch
+    parts = [scenes.uniform(k, ns=3, periods=0.03, seed=40 + k, pa_hi=1.2, x_range=(-0.5, 0.5))
+             for k in (12, 16, 24, 32)]
+    sc = scenes.concat(*parts)
+    ens, models = Ensemble.from_scene(sc, return_models=True)
+    ens.to_device()
+    ens.solve(100_000)
+    torch.cuda.synchronize()
+    gpu = ens.to_host()
+    ref = oracle_ragged(models, ens.host, 100_000, ens.solver_spec)
+    compare(gpu, ref)
+    assert np.all(gpu["status"] != 0)
+
+
 def test_graph_replay_and_dense_grid(cuda):
     """Replaying a plan on reset inputs reproduces the same results; grid-mode
     dense output in the sample-major layout matches the oracle."""

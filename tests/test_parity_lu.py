@@ -25,7 +25,7 @@ def test_lu_bit_exact_small_k(cuda, K):
     assert int(gpu["convergence_failures"].sum()) == 0
 
 
-@pytest.mark.parametrize("K", [12, 16, 32])
+@pytest.mark.parametrize("K", [12, 16, 24, 32])
 def test_lu_bit_exact_large_k(cuda, K):
     sc = scenes.uniform(K, ns=6, periods=0.05, seed=50 + K, pa_hi=1.2, x_range=(-0.5, 0.5), samples_per_period=40)
     gpu, ref = run_pair(sc, solver_spec=LU)

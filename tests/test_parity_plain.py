@@ -26,8 +26,9 @@ def test_bit_exact_small_k(cuda, K):
     assert np.all(gpu["status_flags"] != 0)
 
 
-@pytest.mark.parametrize("K", [16, 32])
+@pytest.mark.parametrize("K", [12, 16, 24, 32])
 def test_bit_exact_large_k(cuda, K):
+    # 16 and 32: kernels compiled for that exact K; 12 and 24: run-time K
     sc = scenes.uniform(K, ns=6, periods=0.05, seed=20 + K, pa_hi=1.2, x_range=(-0.5, 0.5))
     gpu, ref = run_pair(sc)
     assert_bit_exact(gpu, ref)
