@@ -666,6 +666,40 @@ def run_b200(args):
         pg.destroy_process_group()
 
 
+def cost_tables(dev_index: int = 0, seconds: float = 0.5):
+    """Per-K cost tables of the adaptive scheduler: the steady cost of one
+    step attempt with the GPU full (ns: the K bucket of the mixed-K workload,
+    a device-time slice of `seconds` from t = 0), the latency of one attempt
+    of a system alone (us) and, from the same slice, the latency one attempt
+    sees inside the full GPU (us, 90th percentile of the systems' attempt
+    counts) over the alone latency (the load factor)."""
+    import torch
+    from cbc_b200 import scenes
+    from cbc_b200.ensemble import Ensemble
+    torch.cuda.set_device(dev_index)
+    mix = scenes.mixed_k(ns=65536, seed=1)
+    one = scenes.uniform(1, ns=26214, periods=20.0, seed=91)
+    step_ns, alone_us, bulk_us = {}, {}, {}
+    for k in (1, 2, 3, 4, 6, 8):
+        sc = one if k == 1 else scenes.subset(mix, np.nonzero(mix.K == k)[0])
+        ens = Ensemble.from_scene(sc, device=dev_index).to_device()
+        ens.solve(200)
+        ens.reset_device()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ens.solve(MAX_STEPS, budget_ns=int(seconds * 1e9))
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        att = (ens.dev["steps"] + ens.dev["rejected"]).cpu().numpy().astype(np.float64)
+        step_ns[k] = ms * 1e6 / float(att.sum())
+        bulk_us[k] = ms * 1e3 / float(np.percentile(att, 90))
+        alone_us[k] = alone_latency(sc if k == 1 else mix, dev_index, "richardson", ks=(k,))[f"K{k}_us_per_attempt"]
+    return {"workload": "cost_tables", "slice_s": seconds, "step_ns": step_ns, "alone_us": alone_us,
+            "bulk_us": bulk_us, "load_factor": {k: bulk_us[k] / alone_us[k] for k in step_ns}}
+
+
 def run_alone(args):
     """Per-attempt latency of single systems alone, both coupling solvers:
     K = 1..8 from the mixed-K workload's distributions, 16 and 32 from
@@ -704,10 +738,11 @@ def main():
                     help="skip the plain parameter study (1,024 x K = 2, 10 periods) through Model.solve")
     ap.add_argument("--no-large-k", dest="large_k", action="store_false",
                     help="skip the large-K dense-output measurement")
-    ap.add_argument("--workload", default="mixed_k", choices=["mixed_k", "alone", "large_k", "served"],
+    ap.add_argument("--workload", default="mixed_k", choices=["mixed_k", "alone", "large_k", "served", "costs"],
                     help="alone: only the single-system step latency of both coupling solvers; large_k: only "
                          "the large-K dense-output measurement (--ns systems of K = 32, --periods); served: "
-                         "only the served streams (20k and 500 req/s, --serve-seconds)")
+                         "only the served streams (20k and 500 req/s, --serve-seconds); costs: the per-K cost "
+                         "tables of the adaptive scheduler")
     ap.add_argument("--periods", type=float, default=0.5, help="span of the large_k workload")
     ap.add_argument("--lin-solver", default="richardson", choices=["richardson", "lu"],
                     help="implicit-coupling solver of the headline arm (richardson: the reference's)")
@@ -735,6 +770,8 @@ def main():
         line = large_k_measure(0, ns=args.ns, periods=args.periods)
         line.update({"metric": METRIC, "n_gpus": 1, "dtype": "f64", "data": "synthetic"})
         print(json.dumps(line), flush=True)
+    elif args.workload == "costs":
+        print(json.dumps(cost_tables(0)), flush=True)
     elif args.workload == "served":
         import torch
         torch.cuda.set_device(0)

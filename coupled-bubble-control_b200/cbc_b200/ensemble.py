@@ -39,12 +39,13 @@ class WorkList:
     min_blocks: Optional[np.ndarray] = None  # (nb,) int32 register-budget variant 0 / 1 (autotuner)
 
 
-# Steady-state cost of one step attempt on a full B200 (ns), measured on
-# uniform-K ensembles with every slot busy (no tail); other K are interpolated.
-STEP_NS = {1: 0.50, 2: 0.714, 3: 1.83, 4: 2.27, 6: 6.49, 8: 8.18}
+# Steady-state cost of one step attempt on a full B200 (ns), measured on the
+# K buckets of the mixed-K workload filling the GPU (a 0.5 s slice from t = 0;
+# `python bench.py --workload costs`); other K are interpolated.
+STEP_NS = {1: 0.58, 2: 0.846, 3: 2.14, 4: 2.55, 6: 6.32, 8: 7.16}
 # Latency of one step attempt of a system whose warp has an SM sub-partition
 # to itself (us), measured on single systems of the mixed-K workload.
-ALONE_US = {1: 16.0, 2: 18.3, 3: 20.5, 4: 22.4, 6: 27.0, 8: 29.6}
+ALONE_US = {1: 9.3, 2: 13.9, 3: 15.8, 4: 14.8, 6: 23.5, 8: 23.9}
 
 
 def cost_weight(K) -> np.ndarray:
@@ -363,7 +364,7 @@ class Ensemble:
         return Plan(self, max_steps, work)
 
     def adaptive_plan(self, max_steps: int = 1_000_000, slices=(1.0, 2.0, 4.0, 8.0),
-                      max_lane_sms: int = 32, load_factor: float = 1.45, solo: int = 0) -> "AdaptivePlan":
+                      max_lane_sms: int = 32, load_factor: float = 1.35, solo: int = 0) -> "AdaptivePlan":
         if not self.dev:
             self.to_device()
         return AdaptivePlan(self, max_steps, slices, max_lane_sms, load_factor, solo)
@@ -497,7 +498,7 @@ def lane_work_list(wl: WorkList, K: np.ndarray, lane_ids: np.ndarray, order_key:
 
 
 def adaptive_work_list(K, t_end, t0, a0, t, attempts, active, sm_count: int, max_lane_sms: int = 32,
-                       load_factor: float = 1.45, min_observed: int = 256, solo: int = 0):
+                       load_factor: float = 1.35, min_observed: int = 256, solo: int = 0):
     """One re-planning step of ``AdaptivePlan`` (host only): the work list
     for the systems still running, from the progress since the solve began
     (t0 / a0: simulated time and step attempts then; t / attempts: now).
@@ -560,8 +561,9 @@ class AdaptivePlan:
       simulated time x its remaining span (the median rate of its K while it
       has not run enough steps to measure its own);
     * a system whose remaining attempts at the latency it sees outside a lane
-      (its alone latency ``ALONE_US`` x ``load_factor``: steady cost per
-      attempt x systems in flight / alone latency = 1.42-1.48 on a full B200)
+      (its alone latency ``ALONE_US`` x ``load_factor``: latency of one
+      attempt inside the full GPU / alone latency = 1.31-1.48 for K = 3..8 on
+      a full B200, ``bench.py --workload costs``)
       exceed the predicted bulk time would end last: it goes to a latency
       lane (an SM of its own, ``cbc_work.exclusive``), longest first, up to
       ``max_lane_sms`` SMs;
@@ -575,7 +577,7 @@ class AdaptivePlan:
     MIN_OBSERVED = 256   # attempts before a system's own rate is trusted
 
     def __init__(self, ens: Ensemble, max_steps: int, slices=(1.0, 2.0, 4.0, 8.0), max_lane_sms: int = 32,
-                 load_factor: float = 1.45, solo: int = 0):
+                 load_factor: float = 1.35, solo: int = 0):
         self.ens = ens
         self.max_steps = int(max_steps)
         self.slices = [float(s) for s in slices]
