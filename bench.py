@@ -37,7 +37,7 @@ import numpy as np  # noqa: E402
 
 METRIC = "system-periods/s @rtol 1e-9, batched vs plain; p50/p99 env-step latency"
 # DRAM traffic of the dominant kernel per launch (ncu, see roofline.traffic_note)
-TRAFFIC_K8_BYTES = 20103680
+TRAFFIC_K8_BYTES = 20219904    # 20,158,720 read + 61,184 written
 UNIT = "system-periods/s"
 MAX_STEPS = 1_000_000
 
