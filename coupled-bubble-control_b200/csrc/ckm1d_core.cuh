@@ -4,8 +4,10 @@
 // consecutive lanes of a warp ("group"); a warp holds floor(32/K) systems.
 // Everything that couples bubbles (coupling terms, the implicit-coupling
 // iteration, reductions for norms, error ratio and the collision event) is
-// exchanged with full-warp __shfl_sync inside the group, so no block barrier
-// and no shared-memory atomics are needed (the reference synchronises the
+// exchanged inside the warp -- full-warp __shfl_sync, or per-warp
+// shared-memory records ordered by __syncwarp (partner states; the iterates
+// for K > 8) -- so no block barrier and no shared-memory atomics are needed
+// (the reference synchronises the
 // whole block 4x per Richardson iteration, ckm1d_def.py:303-404).  Control flow
 // that contains shuffles is warp-uniform; per-system decisions only select
 // values.  Per-system scalars (t, h, event value, ...) are held redundantly by
