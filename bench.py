@@ -255,11 +255,14 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+ADAPTIVE_OPTS = {}   # slices / load_factor of the adaptive schedule (command line)
+
+
 def make_plan(ens, schedule: str, max_steps: int = MAX_STEPS):
     """adaptive: time slices with re-planning and latency lanes; pilot: one
     measured re-ordering after a short pilot pass; span: longest span first."""
     if schedule == "adaptive":
-        return ens.adaptive_plan(max_steps)
+        return ens.adaptive_plan(max_steps, **ADAPTIVE_OPTS)
     if schedule == "pilot":
         return ens.scheduled_plan(max_steps, pilot_steps=min(256, max_steps - 1))
     return ens.plan(max_steps)
@@ -637,7 +640,12 @@ def run_b200(args):
                                  "peak = cuBLAS FP64 GEMM measured in this run"},
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
+            "step_ms": [round(float(x), 1) for x in kern_ms],
         }
+        hist = getattr(plan, "history", None)
+        if hist:
+            line["schedule_last_solve"] = [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in h.items()}
+                                          for h in hist]
         if plain:
             line["plain"] = plain
             line["batched_vs_plain"] = plain["batched_same_systems"] / plain["value"]
@@ -757,11 +765,20 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--max-steps", type=int, default=MAX_STEPS,
                     help="step cap per system (the reference's max_steps); small values make short profiling cases")
+    ap.add_argument("--slices", default="",
+                    help="device-time slices (s) of the adaptive schedule before its last, unbounded one, "
+                         "comma separated (default 1,2,4,8)")
+    ap.add_argument("--load-factor", type=float, default=0.0,
+                    help="latency-lane criterion of the adaptive schedule (0: the default)")
     ap.add_argument("--schedule", default="adaptive", choices=["adaptive", "pilot", "span"],
                     help="pilot: measured longest-first re-ordering after a pilot pass; span: longest span first")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.slices:
+        ADAPTIVE_OPTS["slices"] = tuple(float(x) for x in args.slices.split(","))
+    if args.load_factor > 0:
+        ADAPTIVE_OPTS["load_factor"] = args.load_factor
     if args.workload == "alone":
         run_alone(args)
     elif args.workload == "large_k":

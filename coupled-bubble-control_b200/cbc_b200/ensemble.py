@@ -364,7 +364,7 @@ class Ensemble:
         return Plan(self, max_steps, work)
 
     def adaptive_plan(self, max_steps: int = 1_000_000, slices=(1.0, 2.0, 4.0, 8.0),
-                      max_lane_sms: int = 32, load_factor: float = 1.35, solo: int = 0) -> "AdaptivePlan":
+                      max_lane_sms: int = 32, load_factor: float = 1.2, solo: int = 0) -> "AdaptivePlan":
         if not self.dev:
             self.to_device()
         return AdaptivePlan(self, max_steps, slices, max_lane_sms, load_factor, solo)
@@ -498,7 +498,7 @@ def lane_work_list(wl: WorkList, K: np.ndarray, lane_ids: np.ndarray, order_key:
 
 
 def adaptive_work_list(K, t_end, t0, a0, t, attempts, active, sm_count: int, max_lane_sms: int = 32,
-                       load_factor: float = 1.35, min_observed: int = 256, solo: int = 0):
+                       load_factor: float = 1.2, min_observed: int = 256, solo: int = 0):
     """One re-planning step of ``AdaptivePlan`` (host only): the work list
     for the systems still running, from the progress since the solve began
     (t0 / a0: simulated time and step attempts then; t / attempts: now).
@@ -561,9 +561,11 @@ class AdaptivePlan:
       simulated time x its remaining span (the median rate of its K while it
       has not run enough steps to measure its own);
     * a system whose remaining attempts at the latency it sees outside a lane
-      (its alone latency ``ALONE_US`` x ``load_factor``: latency of one
-      attempt inside the full GPU / alone latency = 1.31-1.48 for K = 3..8 on
-      a full B200, ``bench.py --workload costs``)
+      (its alone latency ``ALONE_US`` x ``load_factor``; the latency of one
+      attempt inside the full GPU is 1.31-1.48x the alone latency for
+      K = 3..8 on a full B200, ``bench.py --workload costs``, but 1.2 gave
+      the shortest mixed-K solves of 1.0-1.35: every lane takes a whole SM
+      from the bulk)
       exceed the predicted bulk time would end last: it goes to a latency
       lane (an SM of its own, ``cbc_work.exclusive``), longest first, up to
       ``max_lane_sms`` SMs;
@@ -577,7 +579,7 @@ class AdaptivePlan:
     MIN_OBSERVED = 256   # attempts before a system's own rate is trusted
 
     def __init__(self, ens: Ensemble, max_steps: int, slices=(1.0, 2.0, 4.0, 8.0), max_lane_sms: int = 32,
-                 load_factor: float = 1.35, solo: int = 0):
+                 load_factor: float = 1.2, solo: int = 0):
         self.ens = ens
         self.max_steps = int(max_steps)
         self.slices = [float(s) for s in slices]
