@@ -31,7 +31,7 @@ def test_adaptive_replanning_host_logic():
     systems that would end last go to latency lanes (longest first, inside
     the SM budget), every active system appears exactly once, finished ones
     not at all."""
-    from cbc_b200.ensemble import adaptive_work_list
+    from cbc_b200.ensemble import adaptive_work_list, alone_latency
     rng = np.random.default_rng(5)
     n = 3000
     K = rng.choice([2, 3, 4, 6, 8], size=n)
@@ -49,7 +49,8 @@ def test_adaptive_replanning_host_logic():
     assert info["lane_systems"] > 0 and 1 <= info["lane_sms"] <= 8
     lanes = [b for b in range(wl.bucket_K.size) if wl.exclusive[b] > 0]
     in_lane = set(np.concatenate([wl.order[wl.bucket_begin[b]:wl.bucket_begin[b + 1]] for b in lanes]).tolist())
-    slow = [i for i in range(5) if t_end[i] * 12000.0 * 1e-6 * 29.6 > 2.0]   # long serial chains
+    # long serial chains: remaining attempts x their alone latency well past the bulk time
+    slow = [i for i in range(5) if (t_end[i] - t[i]) * 12000.0 * alone_latency(K[i])[0] * 1e-6 > 2.0]
     assert set(slow) <= in_lane
     # with no observations yet the fallback rate still yields a complete list
     # inside the default lane budget of 32 SMs
