@@ -410,15 +410,16 @@ def lu_arm(scene, dev_index: int, schedule: str, flush, max_steps: int = MAX_STE
     return out
 
 
-def env_step_latency(dev_index: int, n_steps: int = 128, warmup: int = 3):
+def env_step_latency(dev_index: int, n_steps: int = 128, warmup: int = 3, envs_per_warp: int = -1):
     """PPO vec-env stepping: 1024 envs x K=4 bubbles (R0 60 um, SW_N, 25+50 kHz),
     5 periods per env step, actions (PA_1, PA_2) ~ U[0, 1.5] bar from seed 2,
     float32 observation written in place, 128-step horizon with resets.
     Returns p50/p95/p99 of the env-step time measured with CUDA events."""
     import torch
     from cbc_b200.envs import CKM1DVecEnv
+    kw = {} if envs_per_warp < 0 else {"envs_per_warp": envs_per_warp}
     env = CKM1DVecEnv(num_envs=1024, num_bubbles=4, time_step_length=5.0, episode_length=128, seed=42,
-                      device=dev_index)
+                      device=dev_index, **kw)
     env.reset()
     gen = torch.Generator(device=torch.device("cuda", dev_index)).manual_seed(2)
     times = []

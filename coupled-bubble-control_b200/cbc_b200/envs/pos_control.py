@@ -109,7 +109,7 @@ class CKM1DVecEnv:
                  position_tolerance: float = 0.01, dnorm: float = 0.2, reward_exp: float = 0.5,
                  rewards_weights=(1.0, 0.0), positive_terminal_reward: float = 10.0,
                  negative_terminal_reward: float = -10.0, max_steps: int = 1_000_000,
-                 solver_spec: Optional[SolverSpec] = None, device: int = 0):
+                 solver_spec: Optional[SolverSpec] = None, device: int = 0, envs_per_warp: int = 0):
         import torch
         self.num_envs, self.K = int(num_envs), int(num_bubbles)
         self.time_step_length = float(time_step_length)
@@ -174,6 +174,12 @@ class CKM1DVecEnv:
         io.seed = g.seed
         self._io = io
         wl = make_work_list(self.ens.host["K"], np.full(self.num_envs, self.time_step_length))
+        # envs per warp: 0 packs floor(32 / K).  Fewer leave lanes idle and
+        # free each env from the Richardson sweeps of its warp-mates, but the
+        # extra warps share the SMs' issue slots: 1024 envs of K = 4 stepped
+        # in 68 ms packed, 77 ms at 2 and 87 ms at 1 env per warp
+        if envs_per_warp > 0:
+            wl.slots = np.full(wl.bucket_K.size, min(int(envs_per_warp), 32 // self.K), np.int32)
         self._w, self._keep = self.ens.work(wl)
         self._spec, self._e = self.ens.spec(), self.ens.abi()
         self.ctx = _lib.default_context(device)

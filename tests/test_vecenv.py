@@ -50,6 +50,29 @@ def test_env_step_matches_oracle(cuda):
     env.close()
 
 
+def test_envs_per_warp_bit_identical(cuda):
+    """One env per warp (idle lanes, no shared Richardson loop) gives the
+    same step results as the packed default."""
+    import torch
+    from cbc_b200.envs import CKM1DVecEnv
+    out = []
+    for epw in (0, 1):
+        env = CKM1DVecEnv(num_envs=40, num_bubbles=4, time_step_length=0.05, episode_length=2, seed=9,
+                          envs_per_warp=epw)
+        env.reset()
+        gen = torch.Generator(device="cuda").manual_seed(4)
+        res = []
+        for _ in range(3):
+            obs, rew, term, trunc, info = env.step(torch.rand((40, 2), device="cuda", generator=gen) * 1.5)
+            torch.cuda.synchronize()
+            res.append((obs.cpu().numpy().copy(), rew.cpu().numpy().copy(), env.ens.to_host()["state"].copy()))
+        env.close()
+        out.append(res)
+    for a, b in zip(*out):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
 def _torch_reward(x, targets, failed, actions, tol=0.01, dnorm=0.2, exp=0.5, w=(1.0, 0.0), pos=10.0, neg=-10.0):
     """The reference's reward and termination (get_rewards :792-813,
     check_termination :772-789) in torch float32."""
