@@ -99,7 +99,7 @@ def save_cache(table: Dict[str, dict], path: Optional[str] = None) -> None:
     path = path or cache_path()
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)
-        tmp = path + ".tmp"
+        tmp = f"{path}.{os.getpid()}.tmp"     # one per process: ranks of a job may save at once
         with open(tmp, "w") as f:
             json.dump(table, f, indent=1, sort_keys=True)
         os.replace(tmp, path)
