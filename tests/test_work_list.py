@@ -82,3 +82,39 @@ def test_solo_lanes_keep_every_system_once():
             for b in solo_b:
                 seg = wl.order[wl.bucket_begin[b]:wl.bucket_begin[b + 1]]
                 assert wl.exclusive[b] == (seg.size + 3) // 4 and np.all(K[seg] == wl.bucket_K[b])
+
+
+def test_lane_threshold_monotone():
+    """The latency-lane criterion multiplies a system's serial time by
+    `load_factor`: a larger factor never puts fewer systems into lanes, and
+    the chosen systems are the longest chains."""
+    from cbc_b200.ensemble import adaptive_work_list, alone_latency
+    rng = np.random.default_rng(11)
+    n = 4000
+    K = rng.choice([2, 3, 4, 6, 8], size=n)
+    t_end = rng.uniform(5.0, 50.0, n)
+    t0 = np.zeros(n)
+    t = rng.uniform(0.0, 2.0, n)
+    rate = rng.uniform(500, 3000, n)
+    rate[:40] = rng.uniform(8000, 14000, 40)
+    attempts = (rate * t).astype(np.int64)
+    a0 = np.zeros(n, np.int64)
+    active = np.ones(n, bool)
+    counts = []
+    for lf in (0.8, 1.0, 1.2, 1.35, 1.6, 2.0):
+        wl, info = adaptive_work_list(K, t_end, t0, a0, t, attempts, active, sm_count=148, max_lane_sms=32,
+                                      load_factor=lf)
+        assert sorted(wl.order.tolist()) == list(range(n))
+        counts.append(info["lane_systems"])
+        if info["lane_systems"]:
+            lanes = [b for b in range(wl.bucket_K.size) if wl.exclusive[b] > 0]
+            in_lane = np.concatenate([wl.order[wl.bucket_begin[b]:wl.bucket_begin[b + 1]] for b in lanes])
+            # systems with enough attempts to use their own rate: every lane
+            # system's predicted serial time is at least that of those left out
+            own = attempts >= 256
+            serial = (t_end - t) * (attempts / np.maximum(t, 1e-12)) * alone_latency(K)
+            out = np.setdiff1d(np.nonzero(own)[0], in_lane)
+            lane_own = in_lane[own[in_lane]]
+            if lane_own.size and out.size:
+                assert serial[lane_own].min() >= serial[out].max() * 0.999
+    assert counts == sorted(counts)
