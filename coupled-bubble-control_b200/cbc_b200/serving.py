@@ -42,6 +42,7 @@ import numpy as np
 
 from . import _lib, admission, scenes
 from .admission import RangeAllocator
+from .ensemble import cost_weight
 from .models import SolverSpec, water
 
 
@@ -245,6 +246,15 @@ class SolveServer:
         w.nbuckets = int(bk.size)
         w.bucket_K = bk.ctypes.data
         w.bucket_begin = bb.ctypes.data
+        # every bucket starts with a share of the GPU proportional to the cost
+        # of one step of all its systems: without shares each bucket's grid
+        # asks for the whole GPU, and whichever kernel's blocks reach the SMs
+        # first holds them for the slice
+        sh = None
+        if bk.size > 1:
+            c = np.diff(bb).astype(np.float64) * cost_weight(bk)
+            sh = (c / c.sum()).astype(np.float32)
+            w.share = sh.ctypes.data
         if self.chunk_steps > 0:
             max_steps, w.steps_total = self.chunk_steps, 0
         else:
