@@ -5,12 +5,17 @@ coupled-bubble system advanced by one period of the 25 kHz reference drive.
 Workload at N=1: the mixed-K batched ensemble -- 65,536 systems, K in
 {2,3,4,6,8} (p .4/.2/.2/.1/.1), spans U[5,50] periods, water, dual-frequency
 standing wave (25 + 50 kHz), FP64, seeded synthetic inputs (no dataset exists).
-A step is one batched solve of the whole ensemble (one CUDA-graph launch of
-the persistent work-stealing kernels) starting from the same initial state.
+A step is one batched solve of the whole ensemble starting from the same
+initial state: the adaptive schedule (the persistent work-stealing kernels
+in device-time slices, the host re-planning buckets and latency lanes between
+slices; `--schedule span` makes it one CUDA-graph launch).
 
-Also measured (once, outside the timed steps): the plain one-launch-per-K
-reference-layout path on the same ensemble (the reference's execution model:
-one (NS, K) kernel per K, relaunched every 2048 steps with a host check).
+Also measured in the 1-GPU job (outside the timed steps): the plain
+one-launch-per-K reference-layout path on the same ensemble (the reference's
+execution model: one (NS, K) kernel per K, relaunched every 2048 steps with a
+host check), the direct coupling solve, the vec-env step latency, the served
+streams, the large-K dense output, the plain parameter study and the CPU
+oracle.  `--workload alone | large_k | served | costs` runs one of them alone.
 
 Multi-GPU (torchrun): weak scaling, every rank solves its own 65,536-system
 ensemble (seed + rank); no collective on the data path, only the final
