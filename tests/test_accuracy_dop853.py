@@ -15,10 +15,11 @@ backends/numba/sysmtem_definitions/ckm1d_def.py), written as plain numpy
 expressions in natural order: it shares no code and no operation order with
 the kernels or the oracle.
 
-Observed over half a period (3 plain-study K = 2 systems, 3 mixed-K K = 4
-systems; 3,600-13,200 oracle steps, dR/dt changing by up to 41 on the way):
-R within 2.3e-12, x within 1.7e-14, dR/dt within 9.3e-10, dx/dt within
-5.4e-13 (relative, with the floors below).  The bound asserted is 1e-8.
+Observed (3 systems each: plain study K = 2 and mixed-K K = 4 over half a
+period, SW_A; K = 8 SW_N over 0.3 period; K = 3 CONST over half a period;
+3,000-13,200 oracle steps, dR/dt changing by up to 41 on the way): R within
+2.3e-12, x within 1.7e-14, dR/dt within 9.3e-10, dx/dt within 5.4e-13
+(relative, with the floors below).  The bound asserted is 1e-8.
 """
 import copy
 
@@ -118,14 +119,18 @@ def _oracle_tight(scene):
     return start, buf, ms.nk, ms.ac
 
 
-@pytest.mark.parametrize("case", ["plain_K2", "mixed_K4"])
+@pytest.mark.parametrize("case", ["plain_K2", "mixed_K4", "swn_K8", "const_K3"])
 def test_tight_reference_agrees_with_dop853(case):
     if case == "plain_K2":
         sc = scenes.subset(scenes.plain_study(ns=1024, periods=0.5, seed=0), np.arange(3))
-    else:
+    elif case == "mixed_K4":
         mk = scenes.mixed_k(ns=65536, seed=1)
         sc = scenes.subset(mk, np.nonzero(mk.K == 4)[0][:3])
         sc.t_end = np.minimum(sc.t_end, 0.5)
+    elif case == "swn_K8":
+        sc = scenes.uniform(8, ns=3, periods=0.3, seed=21, ac="SW_N")
+    else:
+        sc = scenes.uniform(3, ns=3, periods=0.5, seed=22, ac="CONST")
     start, tight, nk, ac = _oracle_tight(sc)
     K = int(sc.K[0])
     checked = 0
