@@ -1,0 +1,53 @@
+"""The Richardson convergence failures (status -3) of the benchmark workload
+are failures of the physics, not of the linear solver: on systems of the
+mixed-K ensemble (seed 1) that end with -3, the direct coupling solve
+(lin_solver = "lu") stops at the same simulated time with the step-size
+limit (-2), and at that time one bubble of the system has reached the Mach
+singularity of the Keller-Miksis model: its wall speed equals the speed of
+sound (unit constant 7 is 1/c in the model's units, so up7 * dR/dt = 1), the
+radial equation's denominator R (1 - dR/dt / c) + 4 mu / (rho c) (unit
+constants 4 and 7) vanishes and the adaptive step collapses to ~1e-17.  In
+each case this happens at the rebound of a violent collapse (R = 0.12-0.57
+R0, the wall moving outward at the speed of sound).
+
+The systems were found by integrating the first 160 K = 2 and K = 3 systems
+of the workload with the oracle; they fail within the first 0.3-2.3 periods.
+"""
+import numpy as np
+import pytest
+
+from cbc_b200 import scenes
+from cbc_b200.models import SolverSpec
+from oracle import oracle
+
+FAILING = {2: [115, 116, 370], 3: [45, 144, 428]}    # system ids in mixed_k(seed=1)
+
+
+@pytest.fixture(scope="module")
+def workload():
+    return scenes.mixed_k(ns=65536, seed=1)
+
+
+@pytest.mark.parametrize("K", sorted(FAILING))
+def test_convergence_failures_are_mach_singularities(workload, K):
+    sc = scenes.subset(workload, np.asarray(FAILING[K]))
+    assert np.all(sc.K == K)
+    out = {}
+    for lin in ("richardson", "lu"):
+        m = scenes.build_model(sc, solver_spec=SolverSpec(lin_solver=lin), ndo=0)
+        out[lin] = oracle.solve_model(m, max_steps=300_000, kernel_steps=300_000, nthreads=3)
+    ri, lu = out["richardson"], out["lu"]
+    assert np.all(ri["status_flags"] == -3)
+    assert np.all(lu["status_flags"] == -2)
+    # both stop at the same simulated time, with a collapsed step
+    assert np.allclose(ri["actual_time"], lu["actual_time"], rtol=1e-6, atol=0.0)
+    assert np.all(ri["time_step"] < 1e-15) and np.all(lu["time_step"] < 1e-15)
+    up = ri["unit_params"]
+    for s in range(sc.ns):
+        R = ri["actual_state"][0, s, :K]
+        U = ri["actual_state"][2, s, :K]
+        mach = up[7, s, :K] * U                             # dR/dt / c
+        D = R - mach * R + up[4, s, :K] * up[7, s, :K]
+        b = int(np.argmax(mach))
+        assert abs(mach[b] - 1.0) < 0.01, (s, mach)
+        assert abs(D[b]) < 1e-3 * R[b], (s, D, R)
