@@ -51,3 +51,25 @@ def test_convergence_failures_are_mach_singularities(workload, K):
         b = int(np.argmax(mach))
         assert abs(mach[b] - 1.0) < 0.01, (s, mach)
         assert abs(D[b]) < 1e-3 * R[b], (s, D, R)
+
+
+# systems of mixed_k(seed=1) that end with the step-size limit (-2) or a
+# non-finite candidate (-4) under the reference's Richardson solve
+OTHER = {(2, -2): [309, 14], (2, -4): [256], (4, -2): [753, 208], (4, -4): [472, 51]}
+
+
+@pytest.mark.parametrize("key", sorted(OTHER))
+def test_other_failures_are_mach_singularities(workload, key):
+    """The step-size-limit (-2) and non-finite (-4) endings sit at the same
+    singularity: one bubble's wall speed at the speed of sound."""
+    K, code = key
+    sc = scenes.subset(workload, np.asarray(OTHER[key]))
+    assert np.all(sc.K == K)
+    m = scenes.build_model(sc, ndo=0)
+    b = oracle.solve_model(m, max_steps=300_000, kernel_steps=300_000, nthreads=2)
+    assert np.all(b["status_flags"] == code)
+    up = b["unit_params"]
+    for s in range(sc.ns):
+        mach = up[7, s, :K] * b["actual_state"][2, s, :K]
+        assert np.all(np.isfinite(b["actual_state"][:, s, :K]))
+        assert abs(np.max(mach) - 1.0) < 0.02, (s, mach)
